@@ -1,0 +1,807 @@
+// C ABI of the B200 MPS engine (include/vqemps.h): circuit compilation, the
+// shared-prefix plan of a Pauli sum, workspaces and kernel launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/vqemps.h"
+#include "common.cuh"
+#include "evolve.cuh"
+#include "expect.cuh"
+#include "sample.cuh"
+#include "gradient.cuh"
+
+using namespace vqemps;
+
+namespace {
+
+struct Hamiltonian {
+  int n = 0, T = 0;
+  int nleaf = 0;
+  int identity_leaf = -1;
+  bool all_diagonal = true;
+  std::vector<int32_t> term_leaf;        // T
+  std::vector<double> leaf_coef;         // nleaf
+  std::vector<int> group_off, node_off;  // n + 1 offsets into the flat arrays
+  std::vector<int> nslot;                // env slots per level
+  std::vector<DevGroup> groups;
+  std::vector<DevNode> nodes;
+  std::vector<int32_t> leaf_level;       // level of every leaf (-1: identity)
+  int max_slot = 1;
+  // work accounting (FP64 real flops of one evaluation of one state)
+  double flops = 0.0;
+  double flops_survey = 0.0;
+  long long node_sites = 0;
+  // sampling support: Z masks over sites (one uint64 row per word), X/Y flags
+  std::vector<uint64_t> zmask;           // T x W
+  std::vector<uint8_t> offdiag;          // T
+  std::vector<uint8_t> codes;            // T x n site-order Pauli codes
+  std::vector<double> coeffs;            // T
+  int nzwords = 0;                       // non-identity I/Z words (independent streams)
+  // device copies
+  DevGroup *d_groups = nullptr;
+  DevNode *d_nodes = nullptr;
+  double *d_leaf_coef = nullptr;
+  int32_t *d_term_leaf = nullptr;
+  uint64_t *d_zmask = nullptr;
+  uint8_t *d_offdiag = nullptr;
+  uint8_t *d_codes = nullptr;
+  double *d_coeffs = nullptr;
+  int32_t *d_sumidx_shared = nullptr;    // T: t for I/Z words, -1 for X/Y words
+  int32_t *d_sumidx_word = nullptr;      // T: list position, -2 identity, -1 X/Y
+  int32_t *d_wordlist = nullptr;         // nzwords word ids then nzwords last sites
+  ~Hamiltonian() {
+    cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_leaf_coef); cudaFree(d_term_leaf);
+    cudaFree(d_zmask); cudaFree(d_offdiag); cudaFree(d_codes); cudaFree(d_coeffs);
+    cudaFree(d_sumidx_shared); cudaFree(d_sumidx_word); cudaFree(d_wordlist);
+  }
+};
+
+template <typename T>
+struct DevBuf {
+  T *ptr = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t count) {
+    if (count <= cap) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr; cap = 0;
+    cudaError_t e = cudaMalloc(&ptr, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) cap = count;
+    return e;
+  }
+  void release() { if (ptr) cudaFree(ptr); ptr = nullptr; cap = 0; }
+};
+
+}  // namespace
+
+struct vqemps_ctx {
+  int device = 0;
+  int max_bond = 16;
+  double abs_cut = 0.0, rel_cut = 0.0;
+  std::string err;
+  // circuit
+  int n = 0, P = 0, site_order = 0;
+  bool have_circuit = false;
+  bool doubling_ok = false;             // only adjacent CX two-qubit gates (gradient path)
+  std::vector<DevGate> gates;
+  std::vector<cplx> mats;
+  std::vector<int> bonds;               // zero-cutoff allocation bound, n + 1
+  std::vector<int> site_of_qubit;
+  cplx init0, init1;
+  std::vector<GradOp> grad_ops;         // op list of the bond-doubling (gradient) path
+  std::vector<SiteEvent> site_events;   // per-site event lists (gradient path)
+  std::vector<int32_t> ev_off, ev_dims, slot_off, slot_list;
+  int nslots = 0;
+  DevGate *d_gates = nullptr;
+  cplx *d_mats = nullptr;
+  SiteEvent *d_events = nullptr;
+  int32_t *d_ev_off = nullptr, *d_ev_dims = nullptr, *d_slot_off = nullptr, *d_slot_list = nullptr;
+  // hamiltonians
+  std::map<int, std::unique_ptr<Hamiltonian>> hams;
+  int next_handle = 1;
+  // workspaces
+  DevBuf<cplx> sites, right, env0, env1;
+  DevBuf<int32_t> bonds_ws, status;
+  DevBuf<double> leafval, theta_stage, energy_stage, per_term_stage;
+  DevBuf<uint64_t> bits, seeds;
+  DevBuf<int32_t> zsum;
+  DevBuf<cplx> branch;
+  DevBuf<double> analytic_stage;
+  DevBuf<cplx> grad_sites, grad_envs, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
+  DevBuf<double> grad_stage;
+  int last_B = 0;
+  ~vqemps_ctx() {
+    cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
+    cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
+  }
+};
+
+static int fail(vqemps_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, expr)                                                          \
+  do {                                                                               \
+    cudaError_t _e = (expr);                                                         \
+    if (_e != cudaSuccess)                                                           \
+      return fail(ctx, VQEMPS_CUDA_ERROR, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+static cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+static bool build_site_events(vqemps_ctx *ctx);
+static int upload_site_events(vqemps_ctx *ctx);
+
+// ---------------------------------------------------------------------------
+// creation
+// ---------------------------------------------------------------------------
+extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double rel_cut,
+                             vqemps_ctx **out) {
+  if (!out) return VQEMPS_INVALID;
+  *out = nullptr;
+  if (max_bond < 1 || max_bond > CHI) return VQEMPS_INVALID;
+  if (!(abs_cut >= 0.0) || !(rel_cut >= 0.0)) return VQEMPS_INVALID;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    return VQEMPS_CUDA_ERROR;
+  if (cudaSetDevice(device) != cudaSuccess) return VQEMPS_CUDA_ERROR;
+  auto *ctx = new vqemps_ctx();
+  ctx->device = device;
+  ctx->max_bond = max_bond;
+  ctx->abs_cut = abs_cut;
+  ctx->rel_cut = rel_cut;
+  cudaFuncSetAttribute(evolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelSmem));
+  grad_set_attributes();
+  *out = ctx;
+  return VQEMPS_OK;
+}
+
+extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
+  if (!ctx) return VQEMPS_OK;
+  cudaSetDevice(ctx->device);
+  ctx->hams.clear();
+  ctx->sites.release(); ctx->right.release(); ctx->env0.release(); ctx->env1.release();
+  ctx->bonds_ws.release(); ctx->status.release(); ctx->leafval.release();
+  ctx->theta_stage.release(); ctx->energy_stage.release(); ctx->per_term_stage.release();
+  ctx->bits.release(); ctx->zsum.release(); ctx->seeds.release(); ctx->branch.release();
+  ctx->analytic_stage.release();
+  ctx->grad_sites.release(); ctx->grad_envs.release(); ctx->grad_bar0.release();
+  ctx->grad_bar1.release(); ctx->grad_sitebar.release(); ctx->grad_stage.release();
+  ctx->grad_partial.release(); ctx->grad_leafsum.release();
+  delete ctx;
+  return VQEMPS_OK;
+}
+
+extern "C" const char *vqemps_last_error(const vqemps_ctx *ctx) {
+  if (!ctx) return "null context";
+  return ctx->err.c_str();
+}
+
+// ---------------------------------------------------------------------------
+// circuit compilation
+// ---------------------------------------------------------------------------
+static void push_matrix(std::vector<cplx> &mats, const cplx *m, int count, int *offset) {
+  *offset = (int)mats.size();
+  for (int i = 0; i < count; ++i) mats.push_back(m[i]);
+}
+
+extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, int nops,
+                                  const double *matrices, int nmatrices, int initial,
+                                  int site_order) {
+  if (!ctx) return VQEMPS_INVALID;
+  if (n < 2) return fail(ctx, VQEMPS_INVALID, "the MPS engine needs >= 2 qubits");
+  if (nops < 0 || (nops > 0 && !ops)) return fail(ctx, VQEMPS_INVALID, "bad op list");
+  if (nmatrices < 0 || (nmatrices > 0 && !matrices)) return fail(ctx, VQEMPS_INVALID, "bad matrix table");
+  if (site_order != 0 && site_order != 1) return fail(ctx, VQEMPS_INVALID, "site_order must be 0 or 1");
+  if (EvolveSmem::bytes(n) > 200 * 1024) return fail(ctx, VQEMPS_INVALID, "too many qubits for one CTA");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const double r2 = 1.0 / std::sqrt(2.0);
+  cplx init0, init1;
+  switch (initial) {
+    case VQEMPS_INIT_ZERO: init0 = cmake(1, 0); init1 = cmake(0, 0); break;
+    case VQEMPS_INIT_ONE: init0 = cmake(0, 0); init1 = cmake(1, 0); break;
+    case VQEMPS_INIT_PLUS: init0 = cmake(r2, 0); init1 = cmake(r2, 0); break;
+    case VQEMPS_INIT_MINUS: init0 = cmake(r2, 0); init1 = cmake(-r2, 0); break;
+    default: return fail(ctx, VQEMPS_INVALID, "unknown initial state");
+  }
+  std::vector<int> site_of(n);
+  for (int q = 0; q < n; ++q) site_of[q] = site_order == 1 ? n - 1 - q : q;
+
+  std::vector<cplx> mats;
+  // fixed one-site matrices: H X Y Z S SDG
+  int fixed_off[6];
+  {
+    const cplx h[4] = {cmake(r2, 0), cmake(r2, 0), cmake(r2, 0), cmake(-r2, 0)};
+    const cplx x[4] = {cmake(0, 0), cmake(1, 0), cmake(1, 0), cmake(0, 0)};
+    const cplx y[4] = {cmake(0, 0), cmake(0, -1), cmake(0, 1), cmake(0, 0)};
+    const cplx z[4] = {cmake(1, 0), cmake(0, 0), cmake(0, 0), cmake(-1, 0)};
+    const cplx sg[4] = {cmake(1, 0), cmake(0, 0), cmake(0, 0), cmake(0, 1)};
+    const cplx sd[4] = {cmake(1, 0), cmake(0, 0), cmake(0, 0), cmake(0, -1)};
+    push_matrix(mats, h, 4, &fixed_off[0]);
+    push_matrix(mats, x, 4, &fixed_off[1]);
+    push_matrix(mats, y, 4, &fixed_off[2]);
+    push_matrix(mats, z, 4, &fixed_off[3]);
+    push_matrix(mats, sg, 4, &fixed_off[4]);
+    push_matrix(mats, sd, 4, &fixed_off[5]);
+  }
+  int swap_off;
+  {
+    cplx sw[16];
+    for (int I = 0; I < 2; ++I)
+      for (int J = 0; J < 2; ++J)
+        for (int i = 0; i < 2; ++i)
+          for (int j = 0; j < 2; ++j)
+            sw[(I * 2 + J) * 4 + (i * 2 + j)] = cmake((I == j && J == i) ? 1 : 0, 0);
+    push_matrix(mats, sw, 16, &swap_off);
+  }
+  std::vector<DevGate> gates;
+  std::vector<GradOp> gops;
+  std::vector<int> bonds(n + 1, 1);
+  int P = 0;
+  bool doubling_ok = true;
+  const int maxb = ctx->max_bond;
+  auto add_two = [&](int s, int mat) {
+    DevGate g{};
+    g.kind = GATE_TWO; g.site = s; g.mat = mat; g.rot = ROT_NONE; g.param = -1; g.angle = 0;
+    gates.push_back(g);
+    bonds[s + 1] = std::min(std::min(2 * bonds[s], 2 * bonds[s + 2]), maxb);
+  };
+  for (int k = 0; k < nops; ++k) {
+    const vqemps_op &op = ops[k];
+    auto bad_q = [&](int q) { return q < 0 || q >= n; };
+    if (op.kind <= VQEMPS_SDG || op.kind == VQEMPS_U1) {
+      if (bad_q(op.q0)) return fail(ctx, VQEMPS_INVALID, "qubit index out of range");
+      DevGate g{};
+      g.kind = GATE_ONE; g.site = site_of[op.q0]; g.param = -1; g.angle = op.angle;
+      g.mat = -1; g.rot = ROT_NONE;
+      GradOp go{};
+      go.kind = GOP_ONE; go.site = g.site; go.param = -1; go.angle = op.angle; go.mat = -1;
+      go.rot = ROT_NONE;
+      if (op.kind <= VQEMPS_RZ) {
+        g.rot = op.kind == VQEMPS_RX ? ROT_X : op.kind == VQEMPS_RY ? ROT_Y : ROT_Z;
+        g.param = op.param;
+        if (op.param >= 0) P = std::max(P, op.param + 1);
+        go.rot = g.rot; go.param = g.param;
+      } else if (op.kind == VQEMPS_U1) {
+        if (op.matrix < 0 || op.matrix + 4 > nmatrices)
+          return fail(ctx, VQEMPS_INVALID, "U1 matrix index out of range");
+        cplx m[4];
+        for (int i = 0; i < 4; ++i) m[i] = cmake(matrices[2 * (op.matrix + i)], matrices[2 * (op.matrix + i) + 1]);
+        push_matrix(mats, m, 4, &g.mat);
+        go.mat = g.mat;
+      } else {
+        g.mat = fixed_off[op.kind - VQEMPS_H];
+        go.mat = g.mat;
+      }
+      gates.push_back(g);
+      gops.push_back(go);
+      continue;
+    }
+    if (op.kind != VQEMPS_CX && op.kind != VQEMPS_U2 && op.kind != VQEMPS_SWAP)
+      return fail(ctx, VQEMPS_INVALID, "unsupported gate kind (>2-qubit or multi-control gates are not supported)");
+    if (bad_q(op.q0) || bad_q(op.q1) || op.q0 == op.q1)
+      return fail(ctx, VQEMPS_INVALID, "bad two-qubit gate operands");
+    cplx g4[16];
+    if (op.kind == VQEMPS_CX) {
+      // controlledGate (simulator_mps_dist.cu:376-384): [(C*2+T)*4 + (c*2+t)]
+      for (int C = 0; C < 2; ++C)
+        for (int T = 0; T < 2; ++T)
+          for (int c = 0; c < 2; ++c)
+            for (int t = 0; t < 2; ++t) {
+              double v = 0;
+              if (C == c) v = (c == 0) ? (T == t ? 1 : 0) : (T != t ? 1 : 0);
+              g4[(C * 2 + T) * 4 + (c * 2 + t)] = cmake(v, 0);
+            }
+    } else if (op.kind == VQEMPS_SWAP) {
+      for (int i = 0; i < 16; ++i) g4[i] = mats[swap_off + i];
+    } else {
+      if (op.matrix < 0 || op.matrix + 16 > nmatrices)
+        return fail(ctx, VQEMPS_INVALID, "U2 matrix index out of range");
+      for (int i = 0; i < 16; ++i)
+        g4[i] = cmake(matrices[2 * (op.matrix + i)], matrices[2 * (op.matrix + i) + 1]);
+    }
+    int a = site_of[op.q0], bsite = site_of[op.q1];
+    if (a > bsite) {  // swapOperands (sharded_mps.cuh:555-562)
+      cplx h4[16];
+      for (int I = 0; I < 2; ++I)
+        for (int J = 0; J < 2; ++J)
+          for (int i = 0; i < 2; ++i)
+            for (int j = 0; j < 2; ++j)
+              h4[(I * 2 + J) * 4 + (i * 2 + j)] = g4[(J * 2 + I) * 4 + (j * 2 + i)];
+      std::memcpy(g4, h4, sizeof(g4));
+      std::swap(a, bsite);
+    }
+    int off;
+    push_matrix(mats, g4, 16, &off);
+    // SWAP routing (sharded_mps.cuh:565-572)
+    for (int x = bsite; x > a + 1; --x) add_two(x - 1, swap_off);
+    add_two(a, off);
+    for (int x = a + 1; x < bsite; ++x) add_two(x, swap_off);
+    if (op.kind == VQEMPS_CX && bsite == a + 1) {
+      GradOp go{};
+      go.kind = GOP_CX; go.site = a;
+      go.param = (site_of[op.q0] == a) ? 0 : 1;   // 0: control on the left site
+      go.mat = -1; go.rot = ROT_NONE; go.angle = 0;
+      gops.push_back(go);
+    } else {
+      doubling_ok = false;
+    }
+  }
+  // upload
+  cudaFree(ctx->d_gates); ctx->d_gates = nullptr;
+  cudaFree(ctx->d_mats); ctx->d_mats = nullptr;
+  CUDA_TRY(ctx, cudaMalloc(&ctx->d_gates, std::max<size_t>(gates.size(), 1) * sizeof(DevGate)));
+  CUDA_TRY(ctx, cudaMalloc(&ctx->d_mats, std::max<size_t>(mats.size(), 1) * sizeof(cplx)));
+  if (!gates.empty())
+    CUDA_TRY(ctx, cudaMemcpy(ctx->d_gates, gates.data(), gates.size() * sizeof(DevGate), cudaMemcpyHostToDevice));
+  CUDA_TRY(ctx, cudaMemcpy(ctx->d_mats, mats.data(), mats.size() * sizeof(cplx), cudaMemcpyHostToDevice));
+  ctx->gates = std::move(gates);
+  ctx->mats = std::move(mats);
+  ctx->grad_ops = std::move(gops);
+  ctx->bonds = bonds;
+  ctx->n = n;
+  ctx->P = P;
+  ctx->site_order = site_order;
+  ctx->site_of_qubit = site_of;
+  ctx->init0 = init0;
+  ctx->init1 = init1;
+  ctx->doubling_ok = doubling_ok;
+  ctx->have_circuit = true;
+  if (ctx->doubling_ok) ctx->doubling_ok = build_site_events(ctx);
+  if (ctx->doubling_ok) {
+    const int rc = upload_site_events(ctx);
+    if (rc) return rc;
+  }
+  // Hamiltonians are bound to a width and site order: drop stale ones.
+  for (auto it = ctx->hams.begin(); it != ctx->hams.end();) {
+    if (it->second->n != n) it = ctx->hams.erase(it);
+    else ++it;
+  }
+  return VQEMPS_OK;
+}
+
+extern "C" int vqemps_num_params(const vqemps_ctx *ctx, int *params) {
+  if (!ctx || !params || !ctx->have_circuit) return VQEMPS_INVALID;
+  *params = ctx->P;
+  return VQEMPS_OK;
+}
+
+extern "C" int vqemps_bond_dims(const vqemps_ctx *ctx, int *dims) {
+  if (!ctx || !dims || !ctx->have_circuit) return VQEMPS_INVALID;
+  for (int i = 0; i <= ctx->n; ++i) dims[i] = ctx->bonds[i];
+  return VQEMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Hamiltonian plan: one prefix trie over the sorted site-order words, each path
+// cut after its term's last non-identity site.
+// ---------------------------------------------------------------------------
+extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const double *coeffs,
+                                      int T, int *handle) {
+  if (!ctx || !handle) return VQEMPS_INVALID;
+  if (!ctx->have_circuit) return fail(ctx, VQEMPS_INVALID, "set a circuit before a Hamiltonian");
+  if (T < 0 || (T > 0 && (!words || !coeffs))) return fail(ctx, VQEMPS_INVALID, "bad word list");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  const int n = ctx->n;
+  auto h = std::make_unique<Hamiltonian>();
+  h->n = n;
+  h->T = T;
+  // site-order codes (buildPauliTermData reverses words for the msb map)
+  std::vector<uint8_t> code((size_t)T * n);
+  std::vector<int> last(T, -1);
+  const int W = (n + 63) / 64;
+  h->zmask.assign((size_t)T * W, 0);
+  h->offdiag.assign(T, 0);
+  for (int t = 0; t < T; ++t) {
+    for (int q = 0; q < n; ++q) {
+      const char c = words[(size_t)t * n + q];
+      uint8_t v;
+      switch (c) {
+        case 'I': v = 0; break;
+        case 'X': v = 1; break;
+        case 'Y': v = 2; break;
+        case 'Z': v = 3; break;
+        default: return fail(ctx, VQEMPS_INVALID, "Invalid analytic Pauli");
+      }
+      const int s = ctx->site_of_qubit[q];
+      code[(size_t)t * n + s] = v;
+      if (v == 3) h->zmask[(size_t)t * W + q / 64] |= (1ULL << (q % 64));
+      if (v == 1 || v == 2) h->offdiag[t] = 1;
+    }
+    for (int s = n - 1; s >= 0; --s)
+      if (code[(size_t)t * n + s] != 0) { last[t] = s; break; }
+    if (!std::isfinite(coeffs[t])) return fail(ctx, VQEMPS_INVALID, "nonfinite coefficient");
+    if (h->offdiag[t]) h->all_diagonal = false;
+  }
+  h->coeffs.assign(coeffs, coeffs + T);
+  std::vector<int32_t> sumidx_shared(T), sumidx_word(T), wl, wlast;
+  for (int t = 0; t < T; ++t) {
+    sumidx_shared[t] = h->offdiag[t] ? -1 : t;
+    if (h->offdiag[t]) { sumidx_word[t] = -1; continue; }
+    if (last[t] < 0) { sumidx_word[t] = -2; continue; }
+    sumidx_word[t] = (int32_t)wl.size();
+    wl.push_back(t);
+    wlast.push_back(last[t]);
+  }
+  h->nzwords = (int)wl.size();
+  wl.insert(wl.end(), wlast.begin(), wlast.end());
+  std::vector<int> order(T);
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [&](int a, int b) {
+    const int c = std::memcmp(&code[(size_t)a * n], &code[(size_t)b * n], n);
+    return c != 0 ? c < 0 : a < b;
+  });
+  h->term_leaf.assign(T, -1);
+  // identity words close against the norm
+  for (int t = 0; t < T; ++t)
+    if (last[t] < 0) {
+      if (h->identity_leaf < 0) {
+        h->identity_leaf = h->nleaf++;
+        h->leaf_coef.push_back(0.0);
+        h->leaf_level.push_back(-1);
+      }
+      h->term_leaf[t] = h->identity_leaf;
+      h->leaf_coef[h->identity_leaf] += coeffs[t];
+    }
+  // level-by-level construction over the sorted order
+  std::vector<int> active;  // words (sorted order) still on a path at this level
+  for (int t : order)
+    if (last[t] >= 0) active.push_back(t);
+  std::vector<int> parent_node(active.size(), -1);   // node id at the previous level
+  std::vector<int> prev_slot;                        // env slot of each node of the previous level
+  h->group_off.assign(n + 1, 0);
+  h->node_off.assign(n + 1, 0);
+  h->nslot.assign(n, 0);
+  const std::vector<int> &bd = ctx->bonds;
+  for (int s = 0; s < n; ++s) {
+    h->group_off[s] = (int)h->groups.size();
+    h->node_off[s] = (int)h->nodes.size();
+    std::vector<int> next_active, next_parent;
+    std::vector<int> node_has_child;
+    int level_nodes = 0;
+    int prev_parent = -2, prev_code = -1, cur_node = -1;
+    // pass 1: node assignment (consecutive words with equal (parent, code) share a node)
+    std::vector<int> node_of(active.size());
+    for (size_t j = 0; j < active.size(); ++j) {
+      const int t = active[j];
+      const int c = code[(size_t)t * n + s];
+      if (parent_node[j] != prev_parent || c != prev_code) {
+        cur_node = level_nodes++;
+        DevNode nd{};
+        nd.code = c; nd.env_slot = -1; nd.leaf = -1;
+        h->nodes.push_back(nd);
+        node_has_child.push_back(0);
+        prev_parent = parent_node[j];
+        prev_code = c;
+      }
+      node_of[j] = cur_node;
+      DevNode &nd = h->nodes[h->node_off[s] + cur_node];
+      if (last[t] == s) {
+        if (nd.leaf < 0) {
+          nd.leaf = h->nleaf++;
+          h->leaf_coef.push_back(0.0);
+          h->leaf_level.push_back(s);
+        }
+        h->term_leaf[t] = nd.leaf;
+        h->leaf_coef[nd.leaf] += coeffs[t];
+      } else {
+        node_has_child[cur_node] = 1;
+        next_active.push_back(t);
+        next_parent.push_back(cur_node);
+      }
+    }
+    // env slots for nodes with descendants
+    int slots = 0;
+    std::vector<int> slot_of(level_nodes, -1);
+    for (int k = 0; k < level_nodes; ++k)
+      if (node_has_child[k]) {
+        slot_of[k] = slots++;
+        h->nodes[h->node_off[s] + k].env_slot = slot_of[k];
+      }
+    h->nslot[s] = slots;
+    h->max_slot = std::max(h->max_slot, slots);
+    // groups: consecutive nodes with the same parent
+    {
+      size_t j = 0;
+      while (j < active.size()) {
+        const int par = parent_node[j];
+        const int first = node_of[j];
+        int lastn = first;
+        while (j < active.size() && parent_node[j] == par) { lastn = node_of[j]; ++j; }
+        DevGroup g{};
+        g.parent_slot = (s == 0) ? -1 : prev_slot[par];
+        g.child_begin = first;
+        g.nchild = lastn - first + 1;
+        g.classes = 0;
+        for (int k = first; k <= lastn; ++k) {
+          const int c = h->nodes[h->node_off[s] + k].code;
+          g.classes |= (c == 0 || c == 3) ? 1 : 2;
+        }
+        h->groups.push_back(g);
+        // flop accounting with the actual bond dims (dl x dr site)
+        const double dl = bd[s], dr = bd[s + 1];
+        h->flops += 8.0 * 2.0 * dl * dl * dr;                               // S_i = E A_i
+        h->flops += ((g.classes & 1) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr;  // I/Z products
+        h->flops += ((g.classes & 2) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr;  // X/Y products
+        h->flops_survey += (lastn - first + 1) * 16.0 * dl * dr * (dl + dr);
+        h->node_sites += lastn - first + 1;
+      }
+    }
+    prev_slot = slot_of;
+    active.swap(next_active);
+    parent_node.swap(next_parent);
+  }
+  h->group_off[n] = (int)h->groups.size();
+  h->node_off[n] = (int)h->nodes.size();
+  // upload
+  auto up = [&](auto *&dst, const auto &vec) -> cudaError_t {
+    using E = typename std::remove_reference<decltype(vec)>::type::value_type;
+    cudaError_t e = cudaMalloc(&dst, std::max<size_t>(vec.size(), 1) * sizeof(E));
+    if (e != cudaSuccess) return e;
+    if (!vec.empty()) e = cudaMemcpy(dst, vec.data(), vec.size() * sizeof(E), cudaMemcpyHostToDevice);
+    return e;
+  };
+  CUDA_TRY(ctx, up(h->d_groups, h->groups));
+  CUDA_TRY(ctx, up(h->d_nodes, h->nodes));
+  CUDA_TRY(ctx, up(h->d_leaf_coef, h->leaf_coef));
+  CUDA_TRY(ctx, up(h->d_term_leaf, h->term_leaf));
+  CUDA_TRY(ctx, up(h->d_zmask, h->zmask));
+  CUDA_TRY(ctx, up(h->d_offdiag, h->offdiag));
+  h->codes = std::move(code);
+  CUDA_TRY(ctx, up(h->d_codes, h->codes));
+  CUDA_TRY(ctx, up(h->d_coeffs, h->coeffs));
+  CUDA_TRY(ctx, up(h->d_sumidx_shared, sumidx_shared));
+  CUDA_TRY(ctx, up(h->d_sumidx_word, sumidx_word));
+  CUDA_TRY(ctx, up(h->d_wordlist, wl));
+  const int id = ctx->next_handle++;
+  ctx->hams[id] = std::move(h);
+  *handle = id;
+  return VQEMPS_OK;
+}
+
+extern "C" int vqemps_free_hamiltonian(vqemps_ctx *ctx, int handle) {
+  if (!ctx) return VQEMPS_INVALID;
+  cudaSetDevice(ctx->device);
+  ctx->hams.erase(handle);
+  return VQEMPS_OK;
+}
+
+// Work statistics of a plan (for benchmarks): flops of one evaluation of one state
+// as executed, the survey-style count (16 Dl Dr (Dl + Dr) per trie node-site),
+// node-sites, groups, leaves.
+extern "C" int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats) {
+  if (!ctx || !stats) return VQEMPS_INVALID;
+  auto it = ctx->hams.find(handle);
+  if (it == ctx->hams.end()) return VQEMPS_INVALID;
+  const Hamiltonian &h = *it->second;
+  stats[0] = h.flops;
+  stats[1] = h.flops_survey;
+  stats[2] = (double)h.node_sites;
+  stats[3] = (double)h.groups.size();
+  stats[4] = (double)h.nleaf;
+  stats[5] = (double)h.max_slot;
+  return VQEMPS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// batched energy
+// ---------------------------------------------------------------------------
+static int ensure_state_ws(vqemps_ctx *ctx, int B) {
+  const int n = ctx->n;
+  CUDA_TRY(ctx, ctx->sites.ensure((size_t)B * n * SITE_ELEMS));
+  CUDA_TRY(ctx, ctx->bonds_ws.ensure((size_t)B * (n + 1)));
+  CUDA_TRY(ctx, ctx->status.ensure((size_t)B));
+  CUDA_TRY(ctx, ctx->right.ensure((size_t)B * (n + 1) * ENV_ELEMS));
+  return VQEMPS_OK;
+}
+
+static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaStream_t st) {
+  EvolveParams ep{};
+  ep.gates = ctx->d_gates;
+  ep.ngates = (int)ctx->gates.size();
+  ep.mats = ctx->d_mats;
+  ep.n = ctx->n;
+  ep.P = ctx->P;
+  ep.theta = theta_dev;
+  ep.sites = ctx->sites.ptr;
+  ep.bonds = ctx->bonds_ws.ptr;
+  ep.status = ctx->status.ptr;
+  ep.init0 = ctx->init0;
+  ep.init1 = ctx->init1;
+  ep.max_bond = ctx->max_bond;
+  ep.abs_cut = ctx->abs_cut;
+  ep.rel_cut = ctx->rel_cut;
+  evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return VQEMPS_OK;
+}
+
+// Identity right environments (and the sampler's branch matrices when branch
+// is non-null); writes the norm into the identity leaf of h when given.
+static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st, cplx *branch) {
+  const int nleaf = h ? std::max(h->nleaf, 1) : 0;
+  if (h) CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
+  right_env_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
+                                               ctx->status.ptr, h ? ctx->leafval.ptr : nullptr,
+                                               nleaf, h ? h->identity_leaf : -1);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return VQEMPS_OK;
+}
+
+// Trie levels and the energy reduction on the prepared states (needs launch_right first).
+static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
+                         double *energies_dev, double *per_term_dev) {
+  const int n = ctx->n;
+  const int nleaf = std::max(h.nleaf, 1);
+  CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
+  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * h.max_slot * ENV_ELEMS));
+  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * h.max_slot * ENV_ELEMS));
+  cplx *envs[2] = {ctx->env0.ptr, ctx->env1.ptr};
+  for (int s = 0; s < n; ++s) {
+    const int ng = h.group_off[s + 1] - h.group_off[s];
+    if (ng == 0) break;
+    LevelParams lp{};
+    lp.sites = ctx->sites.ptr;
+    lp.right = ctx->right.ptr;
+    lp.env_prev = envs[(s + 1) & 1];
+    lp.env_cur = envs[s & 1];
+    lp.groups = h.d_groups + h.group_off[s];
+    lp.nodes = h.d_nodes + h.node_off[s];
+    lp.leafval = ctx->leafval.ptr;
+    lp.ngroups = ng;
+    lp.nslot_prev = s > 0 ? std::max(h.nslot[s - 1], 1) : 1;
+    lp.nslot_cur = std::max(h.nslot[s], 1);
+    lp.nleaf_total = nleaf;
+    lp.n = n;
+    lp.s = s;
+    dim3 grid((ng + LEVEL_WARPS - 1) / LEVEL_WARPS, B);
+    level_kernel<<<grid, LEVEL_WARPS * 32, sizeof(LevelSmem), st>>>(lp);
+    CUDA_TRY(ctx, cudaGetLastError());
+  }
+  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h.d_leaf_coef, h.nleaf,
+                                             h.d_term_leaf, h.T, ctx->status.ptr, energies_dev,
+                                             per_term_dev);
+  CUDA_TRY(ctx, cudaGetLastError());
+  return VQEMPS_OK;
+}
+
+static Hamiltonian *find_ham(vqemps_ctx *ctx, int handle) {
+  auto it = ctx->hams.find(handle);
+  return it == ctx->hams.end() ? nullptr : it->second.get();
+}
+
+extern "C" int vqemps_energy_batch(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,
+                                   double *energies_dev, double *per_term_dev, void *stream) {
+  if (!ctx) return VQEMPS_INVALID;
+  if (!ctx->have_circuit) return fail(ctx, VQEMPS_INVALID, "no circuit");
+  Hamiltonian *h = find_ham(ctx, handle);
+  if (!h) return fail(ctx, VQEMPS_INVALID, "unknown Hamiltonian handle");
+  if (B < 1 || (!theta_dev && ctx->P > 0) || !energies_dev)
+    return fail(ctx, VQEMPS_INVALID, "bad batch arguments");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = as_stream(stream);
+  int rc = ensure_state_ws(ctx, B);
+  if (rc) return rc;
+  rc = launch_evolve(ctx, theta_dev, B, st);
+  if (rc) return rc;
+  rc = launch_right(ctx, h, B, st, nullptr);
+  if (rc) return rc;
+  rc = launch_levels(ctx, *h, B, st, energies_dev, per_term_dev);
+  if (rc) return rc;
+  ctx->last_B = B;
+  return VQEMPS_OK;
+}
+
+// Phase timing of one batched energy call: ms[0] state preparation, ms[1]
+// right environments, ms[2] all trie levels, ms[3] reduction; *launches = kernels
+// launched. Records CUDA events on the stream and synchronises it.
+extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,
+                                     double *ms, int *launches, void *stream) {
+  if (!ctx || !ms || !launches) return VQEMPS_INVALID;
+  Hamiltonian *h = find_ham(ctx, handle);
+  if (!h || B < 1) return fail(ctx, VQEMPS_INVALID, "bad profile arguments");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = as_stream(stream);
+  int rc = ensure_state_ws(ctx, B);
+  if (rc) return rc;
+  CUDA_TRY(ctx, ctx->energy_stage.ensure((size_t)B));
+  cudaEvent_t ev[5];
+  for (auto &e : ev) CUDA_TRY(ctx, cudaEventCreate(&e));
+  CUDA_TRY(ctx, cudaEventRecord(ev[0], st));
+  rc = launch_evolve(ctx, theta_dev, B, st);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaEventRecord(ev[1], st));
+  rc = launch_right(ctx, h, B, st, nullptr);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaEventRecord(ev[2], st));
+  // levels and reduction are launched by launch_levels; time them apart by a
+  // second call of the reduction alone
+  rc = launch_levels(ctx, *h, B, st, ctx->energy_stage.ptr, nullptr);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaEventRecord(ev[3], st));
+  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h->d_leaf_coef, h->nleaf, h->d_term_leaf,
+                                             h->T, ctx->status.ptr, ctx->energy_stage.ptr, nullptr);
+  CUDA_TRY(ctx, cudaGetLastError());
+  CUDA_TRY(ctx, cudaEventRecord(ev[4], st));
+  CUDA_TRY(ctx, cudaEventSynchronize(ev[4]));
+  float t[4];
+  for (int i = 0; i < 4; ++i) CUDA_TRY(ctx, cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]));
+  ms[0] = t[0];
+  ms[1] = t[1];
+  ms[3] = t[3];
+  ms[2] = t[2] - t[3];   // launch_levels includes one reduction
+  int nlev = 0;
+  for (int s = 0; s < ctx->n; ++s)
+    if (h->group_off[s + 1] > h->group_off[s]) ++nlev;
+  *launches = 1 + 1 + nlev + 1;
+  for (auto &e : ev) cudaEventDestroy(e);
+  ctx->last_B = B;
+  return VQEMPS_OK;
+}
+
+extern "C" int vqemps_batch_status(vqemps_ctx *ctx, int32_t *status, int B, void *stream) {
+  if (!ctx || !status || B < 1 || B > ctx->last_B) return VQEMPS_INVALID;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = as_stream(stream);
+  CUDA_TRY(ctx, cudaMemcpyAsync(status, ctx->status.ptr, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  int first = VQEMPS_OK;
+  for (int b = 0; b < B; ++b)
+    if (status[b] != 0) { first = status[b]; break; }
+  if (first == VQEMPS_INSUFFICIENT_BOND)
+    ctx->err = "CUDAQ_MPS_MAX_BOND=" + std::to_string(ctx->max_bond) +
+               " is insufficient for zero-cutoff simulation: resolved singular values would be discarded";
+  else if (first == VQEMPS_NONFINITE_SVD)
+    ctx->err = "Direct MPS SVD failed or produced nonfinite singular values";
+  return first;
+}
+
+extern "C" int vqemps_energy_batch_host(vqemps_ctx *ctx, int handle, const double *theta, int B,
+                                        double *energies, double *per_term, void *stream) {
+  if (!ctx) return VQEMPS_INVALID;
+  if (!ctx->have_circuit) return fail(ctx, VQEMPS_INVALID, "no circuit");
+  Hamiltonian *h = find_ham(ctx, handle);
+  if (!h) return fail(ctx, VQEMPS_INVALID, "unknown Hamiltonian handle");
+  if (B < 1 || (!theta && ctx->P > 0) || !energies) return fail(ctx, VQEMPS_INVALID, "bad batch arguments");
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = as_stream(stream);
+  CUDA_TRY(ctx, ctx->theta_stage.ensure((size_t)B * std::max(ctx->P, 1)));
+  CUDA_TRY(ctx, ctx->energy_stage.ensure((size_t)B));
+  if (per_term) CUDA_TRY(ctx, ctx->per_term_stage.ensure((size_t)B * std::max(h->T, 1)));
+  if (ctx->P > 0)
+    CUDA_TRY(ctx, cudaMemcpyAsync(ctx->theta_stage.ptr, theta, sizeof(double) * B * ctx->P,
+                                  cudaMemcpyHostToDevice, st));
+  int rc = vqemps_energy_batch(ctx, handle, ctx->theta_stage.ptr, B, ctx->energy_stage.ptr,
+                               per_term ? ctx->per_term_stage.ptr : nullptr, stream);
+  if (rc) return rc;
+  CUDA_TRY(ctx, cudaMemcpyAsync(energies, ctx->energy_stage.ptr, sizeof(double) * B,
+                                cudaMemcpyDeviceToHost, st));
+  if (per_term)
+    CUDA_TRY(ctx, cudaMemcpyAsync(per_term, ctx->per_term_stage.ptr, sizeof(double) * B * h->T,
+                                  cudaMemcpyDeviceToHost, st));
+  std::vector<int32_t> status(B);
+  return vqemps_batch_status(ctx, status.data(), B, stream);
+}
+
+extern "C" int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, void *stream) {
+  if (!ctx || !sites_host || b < 0 || b >= ctx->last_B) return VQEMPS_INVALID;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  cudaStream_t st = as_stream(stream);
+  CUDA_TRY(ctx, cudaMemcpyAsync(sites_host, ctx->sites.ptr + (size_t)b * ctx->n * SITE_ELEMS,
+                                sizeof(cplx) * ctx->n * SITE_ELEMS, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(ctx, cudaStreamSynchronize(st));
+  return VQEMPS_OK;
+}
+
+#include "engine_sample.inc"
+#include "engine_grad.inc"

@@ -1,0 +1,341 @@
+// State preparation: apply a compiled gate list to B parameter sets at once.
+//
+// Reference algorithm (test/backend/source):
+//   apply1q / k_apply1qInPlace ........ sharded_mps.cuh:16-26, 465-474
+//   apply2q / k_buildM ................ sharded_mps.cuh:30-45, 477-516
+//   singleGpuSvdFactors ............... dist_svd.cuh:233-283 (cuSOLVER Zgesvd)
+//   selectDirectSvdRank ............... dist_svd.cuh:194-212 (zero-cutoff rank guard)
+//   packDirectSvdFactors .............. dist_svd.cuh:214-231 (left = U, right = S*Vh)
+//
+// B200 design: one CTA per parameter set walks the whole gate list; nothing
+// returns to the host between gates (the reference synchronises twice per
+// gate). One-qubit gates are not applied when they arrive: they accumulate in a
+// per-site 2x2 matrix in shared memory and are folded into the next two-site
+// gate's 4x4 matrix (or applied at the end). Each two-site gate builds
+// Theta = G (A (x) B) (2Dl x 2Dr, <= 32 x 32 complex) in shared memory and
+// factors it with an FP64 one-sided Jacobi SVD that orthogonalises the ROWS of
+// Theta by left unitary rotations: V^H Theta = X with orthogonal rows, so the
+// new left site V[:, kept] is unitary to rounding (no division by small
+// singular values, null directions included) and the right site is the kept
+// rows of X = S * Vh. Rows are kept by descending norm, exactly the gesvd
+// ordering the reference uses.
+#pragma once
+#include "common.cuh"
+
+namespace vqemps {
+
+enum : int32_t { GATE_ONE = 0, GATE_TWO = 1 };
+enum : int32_t { ROT_NONE = -1, ROT_X = 0, ROT_Y = 1, ROT_Z = 2 };
+
+struct DevGate {
+  int32_t kind;   // GATE_ONE / GATE_TWO
+  int32_t site;   // target site (ONE) or left site s of the pair (s, s+1) (TWO)
+  int32_t mat;    // offset of a fixed matrix in the matrix table, or -1 (rotation)
+  int32_t rot;    // ROT_* when mat < 0
+  int32_t param;  // parameter index or -1
+  int32_t pad;
+  double angle;   // constant angle (param < 0) or scale (param >= 0)
+};
+
+struct EvolveParams {
+  const DevGate *gates;
+  int ngates;
+  const cplx *mats;
+  int n;
+  int P;
+  const double *theta;   // B x P
+  cplx *sites;           // B x n x SITE_ELEMS
+  int32_t *bonds;        // B x (n + 1)
+  int32_t *status;       // B
+  cplx init0, init1;     // initial single-qubit state
+  int max_bond;
+  double abs_cut, rel_cut;
+};
+
+constexpr int EVOLVE_THREADS = 256;
+constexpr int JACOBI_MAX_SWEEPS = 40;
+
+// Dynamic shared memory layout (bytes).
+struct EvolveSmem {
+  static constexpr int X = 0;                              // 32 x 32 cplx, [row][col]
+  static constexpr int VT = X + 32 * 32 * 16;              // 32 x 32 cplx, [col][row] of V
+  static constexpr int SA = VT + 32 * 32 * 16;             // site s tile
+  static constexpr int SB = SA + SITE_ELEMS * 16;          // site s+1 tile
+  static constexpr int G = SB + SITE_ELEMS * 16;           // fused 4x4
+  static constexpr int NORM = G + 16 * 16;                 // 32 doubles
+  static constexpr int SIG = NORM + 32 * 8;                // 32 sorted singular values
+  static constexpr int PERM = SIG + 32 * 8;                // 32 ints
+  static constexpr int MISC = PERM + 32 * 4;               // scalars
+  static constexpr int PEND = MISC + 64;                   // n x 4 cplx pending 1q matrices
+  static __host__ __device__ int bytes(int n) { return PEND + n * 4 * 16 + (n + 1) * 4 + 16; }
+};
+
+__device__ __forceinline__ void one_site_matrix(const DevGate &g, const cplx *mats,
+                                                const double *theta_b, cplx m[4]) {
+  if (g.mat >= 0) {
+    for (int i = 0; i < 4; ++i) m[i] = mats[g.mat + i];
+    return;
+  }
+  double ang = g.param >= 0 ? theta_b[g.param] * g.angle : g.angle;
+  double s, c;
+  sincos(0.5 * ang, &s, &c);
+  if (g.rot == ROT_Y) {
+    m[0] = cmake(c, 0); m[1] = cmake(-s, 0); m[2] = cmake(s, 0); m[3] = cmake(c, 0);
+  } else if (g.rot == ROT_X) {
+    m[0] = cmake(c, 0); m[1] = cmake(0, -s); m[2] = cmake(0, -s); m[3] = cmake(c, 0);
+  } else {
+    m[0] = cmake(c, -s); m[1] = cmake(0, 0); m[2] = cmake(0, 0); m[3] = cmake(c, s);
+  }
+}
+
+__global__ void __launch_bounds__(EVOLVE_THREADS)
+evolve_kernel(EvolveParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
+  cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
+  cplx *SA = reinterpret_cast<cplx *>(smem + EvolveSmem::SA);
+  cplx *SB = reinterpret_cast<cplx *>(smem + EvolveSmem::SB);
+  cplx *G = reinterpret_cast<cplx *>(smem + EvolveSmem::G);
+  double *NORM = reinterpret_cast<double *>(smem + EvolveSmem::NORM);
+  double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
+  int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
+  int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
+  double *MISCD = reinterpret_cast<double *>(smem + EvolveSmem::MISC + 16);
+  cplx *PEND = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);
+  int *BOND = reinterpret_cast<int *>(smem + EvolveSmem::PEND + p.n * 4 * 16);
+
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x;
+  const int n = p.n;
+  const double *theta_b = p.theta + (size_t)b * p.P;
+  cplx *sites_b = p.sites + (size_t)b * n * SITE_ELEMS;
+
+  // |init>^n product state, zero padded; identity pending matrices.
+  for (int e = tid; e < n * SITE_ELEMS; e += EVOLVE_THREADS) {
+    int el = e % SITE_ELEMS;
+    cplx v = cmake(0, 0);
+    if (el == 0) v = p.init0;
+    else if (el == CHI) v = p.init1;   // (l=0, p=1, r=0)
+    sites_b[e] = v;
+  }
+  for (int s = tid; s < n; s += EVOLVE_THREADS) {
+    PEND[s * 4 + 0] = cmake(1, 0); PEND[s * 4 + 1] = cmake(0, 0);
+    PEND[s * 4 + 2] = cmake(0, 0); PEND[s * 4 + 3] = cmake(1, 0);
+  }
+  for (int s = tid; s <= n; s += EVOLVE_THREADS) BOND[s] = 1;
+  if (tid == 0) MISC[0] = ST_OK;
+  __syncthreads();
+
+  const double eps = 2.2204460492503131e-16;
+  for (int gi = 0; gi < p.ngates; ++gi) {
+    const DevGate g = p.gates[gi];
+    if (g.kind == GATE_ONE) {
+      if (tid == 0) {
+        cplx m[4];
+        one_site_matrix(g, p.mats, theta_b, m);
+        cplx *u = PEND + g.site * 4;
+        cplx u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
+        u[0] = cadd(cmul(m[0], u0), cmul(m[1], u2));
+        u[1] = cadd(cmul(m[0], u1), cmul(m[1], u3));
+        u[2] = cadd(cmul(m[2], u0), cmul(m[3], u2));
+        u[3] = cadd(cmul(m[2], u1), cmul(m[3], u3));
+      }
+      __syncthreads();
+      continue;
+    }
+    // ---- two-site gate on (s, s+1) ----
+    const int s = g.site;
+    const int dl = BOND[s], dc = BOND[s + 1], dr = BOND[s + 2];
+    const int m = 2 * dl, ncol = 2 * dr;
+    {
+      const cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
+      const cplx *gb = ga + SITE_ELEMS;
+      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) { SA[e] = ga[e]; SB[e] = gb[e]; }
+      if (tid < 16) {
+        // G' = G (U_s (x) U_{s+1}); G'[IJ, ij] = sum_{i'j'} G[IJ, i'j'] U_s[i', i] U_{s+1}[j', j]
+        const int row = tid >> 2, col = tid & 3;
+        const int i = col >> 1, j = col & 1;
+        const cplx *us = PEND + s * 4, *ut = PEND + (s + 1) * 4;
+        cplx acc = cmake(0, 0);
+        for (int ip = 0; ip < 2; ++ip)
+          for (int jp = 0; jp < 2; ++jp)
+            acc = cadd(acc, cmul(p.mats[g.mat + row * 4 + ip * 2 + jp],
+                                 cmul(us[ip * 2 + i], ut[jp * 2 + j])));
+        G[tid] = acc;
+      }
+    }
+    __syncthreads();
+    if (tid < 4) {
+      PEND[s * 4 + tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+      PEND[(s + 1) * 4 + tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+    }
+    // Theta[(l*2+I), (J*dr+r)] = sum_ij G'[(I*2+J)*4+(i*2+j)] sum_c A[l,i,c] B[c,j,r]  (k_buildM)
+    double fro = 0.0;
+    if (tid < dl * dr) {
+      const int l = tid / dr, r = tid % dr;
+      cplx t00 = cmake(0, 0), t01 = cmake(0, 0), t10 = cmake(0, 0), t11 = cmake(0, 0);
+      for (int c = 0; c < dc; ++c) {
+        cplx a0 = SA[(l * 2 + 0) * CHI + c], a1 = SA[(l * 2 + 1) * CHI + c];
+        cplx b0 = SB[(c * 2 + 0) * CHI + r], b1 = SB[(c * 2 + 1) * CHI + r];
+        cfma(t00, a0, b0); cfma(t01, a0, b1); cfma(t10, a1, b0); cfma(t11, a1, b1);
+      }
+      for (int IJ = 0; IJ < 4; ++IJ) {
+        cplx v = cmul(G[IJ * 4 + 0], t00);
+        v = cadd(v, cmul(G[IJ * 4 + 1], t01));
+        v = cadd(v, cmul(G[IJ * 4 + 2], t10));
+        v = cadd(v, cmul(G[IJ * 4 + 3], t11));
+        const int I = IJ >> 1, J = IJ & 1;
+        X[(l * 2 + I) * 32 + (J * dr + r)] = v;
+        fro += cabs2(v);
+      }
+    }
+    // V = identity (stored transposed: VT[col][row])
+    for (int e = tid; e < 32 * 32; e += EVOLVE_THREADS)
+      VT[e] = cmake((e >> 5) == (e & 31) ? 1.0 : 0.0, 0.0);
+    // ||Theta||_F^2 by block reduction
+    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+    if ((tid & 31) == 0) NORM[tid >> 5] = fro;
+    __syncthreads();
+    double total = 0.0;
+    for (int w = 0; w < EVOLVE_THREADS / 32; ++w) total += NORM[w];
+    // Rows below eps * ||Theta||_F are numerically null: pairs whose coupling is
+    // below this floor are left alone, which keeps rank-deficient Theta from
+    // rotating rounding noise forever.
+    const double floor_g = eps * eps * total;
+    const double tol = 4.0 * eps;
+
+    // ---- one-sided Jacobi on the rows of Theta, round-robin pair ordering ----
+    const int pair = tid >> 4, lane = tid & 15;
+    const int npairs = m >> 1;
+    bool converged = (m == 1);
+    for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
+      int rotated = 0;
+      for (int step = 0; step < m - 1; ++step) {
+        int pr = 0, qr = 0;
+        bool active = pair < npairs;
+        if (active) {
+          const int mm1 = m - 1;
+          if (pair == 0) { pr = 0; qr = 1 + (step % mm1); }
+          else { pr = 1 + ((step + pair) % mm1); qr = 1 + ((step + mm1 - pair) % mm1); }
+          if (pr > qr) { int t = pr; pr = qr; qr = t; }
+        }
+        cplx xp0 = cmake(0, 0), xq0 = cmake(0, 0), xp1 = cmake(0, 0), xq1 = cmake(0, 0);
+        const int j0 = lane, j1 = lane + 16;
+        if (active) {
+          if (j0 < ncol) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
+          if (j1 < ncol) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
+        }
+        double al = cabs2(xp0) + cabs2(xp1);
+        double be = cabs2(xq0) + cabs2(xq1);
+        // gamma = sum_j X[p,j] conj(X[q,j])
+        double gr = xp0.x * xq0.x + xp0.y * xq0.y + xp1.x * xq1.x + xp1.y * xq1.y;
+        double gim = xp0.y * xq0.x - xp0.x * xq0.y + xp1.y * xq1.x - xp1.x * xq1.y;
+        for (int o = 8; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o, 16);
+          be += __shfl_xor_sync(0xffffffffu, be, o, 16);
+          gr += __shfl_xor_sync(0xffffffffu, gr, o, 16);
+          gim += __shfl_xor_sync(0xffffffffu, gim, o, 16);
+        }
+        const double ag = sqrt(gr * gr + gim * gim);
+        if (active && ag > floor_g && ag > tol * sqrt(al * be)) {
+          rotated = 1;
+          const double zeta = (be - al) / (2.0 * ag);
+          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+          const double c = 1.0 / sqrt(1.0 + t * t);
+          const double sn = t * c;
+          const cplx e = cmake(gr / ag, gim / ag);          // e^{i phi}
+          const cplx es = cscale(e, sn), ec = cscale(e, c);
+          // X_p' = c X_p - s e X_q ; X_q' = s X_p + c e X_q
+          if (j0 < ncol) {
+            X[pr * 32 + j0] = csub(cscale(xp0, c), cmul(es, xq0));
+            X[qr * 32 + j0] = cadd(cscale(xp0, sn), cmul(ec, xq0));
+          }
+          if (j1 < ncol) {
+            X[pr * 32 + j1] = csub(cscale(xp1, c), cmul(es, xq1));
+            X[qr * 32 + j1] = cadd(cscale(xp1, sn), cmul(ec, xq1));
+          }
+          // V[:,p]' = c V_p - s conj(e) V_q ; V[:,q]' = s V_p + c conj(e) V_q
+          const cplx esc = cconj(es), ecc = cconj(ec);
+          for (int i = lane; i < m; i += 16) {
+            cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
+            VT[pr * 32 + i] = csub(cscale(vp, c), cmul(esc, vq));
+            VT[qr * 32 + i] = cadd(cscale(vp, sn), cmul(ecc, vq));
+          }
+        }
+        __syncthreads();
+      }
+      converged = !__syncthreads_or(rotated);
+    }
+    // ---- singular values = row norms, sorted descending (stable in row index) ----
+    if (tid < m) {
+      double a = 0.0;
+      for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
+      NORM[tid] = sqrt(a);
+    }
+    __syncthreads();
+    if (tid < m) {
+      const double v = NORM[tid];
+      int rank = 0;
+      for (int q = 0; q < m; ++q) {
+        const double w = NORM[q];
+        rank += (w > v) || (w == v && q < tid);
+      }
+      PERM[rank] = tid;
+      SIG[rank] = v;
+    }
+    __syncthreads();
+    // ---- selectDirectSvdRank (dist_svd.cuh:194-212) ----
+    if (tid == 0) {
+      const int r = m < ncol ? m : ncol;
+      int st = converged ? ST_OK : ST_NONFINITE;
+      int selected = 0;
+      const double thr = fmax(p.abs_cut, p.rel_cut * SIG[0]);
+      const bool zero_cut = (p.abs_cut == 0.0 && p.rel_cut == 0.0);
+      for (int i = 0; i < m; ++i)
+        if (!isfinite(NORM[i])) st = ST_NONFINITE;
+      for (int i = 0; i < r; ++i)
+        if (zero_cut || SIG[i] > thr) ++selected;
+      if (st == ST_OK && zero_cut && p.max_bond < r &&
+          SIG[p.max_bond] > 64.0 * eps * r * SIG[0])
+        st = ST_INSUFFICIENT;
+      int k = selected < p.max_bond ? selected : p.max_bond;
+      if (k < 1) k = 1;
+      MISC[0] = st;
+      MISC[1] = k;
+    }
+    __syncthreads();
+    if (MISC[0] != ST_OK) break;
+    const int k = MISC[1];
+    // ---- pack: left = V[:, perm[:k]] (Dl,2,k); right = X[perm[:k], :] (k,2,Dr) ----
+    {
+      cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
+      cplx *gb = ga + SITE_ELEMS;
+      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) {
+        const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
+        ga[e] = (l < dl && c < k) ? VT[PERM[c] * 32 + (l * 2 + I)] : cmake(0, 0);
+        const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
+        gb[e] = (cc < k && r < dr) ? X[PERM[cc] * 32 + (J * dr + r)] : cmake(0, 0);
+      }
+    }
+    if (tid == 0) BOND[s + 1] = k;
+    __syncthreads();
+  }
+  const int status = MISC[0];
+  if (status == ST_OK) {
+    // apply the still-pending one-site matrices in place (apply1q)
+    for (int s = 0; s < n; ++s) {
+      const cplx u0 = PEND[s * 4 + 0], u1 = PEND[s * 4 + 1], u2 = PEND[s * 4 + 2], u3 = PEND[s * 4 + 3];
+      cplx *a = sites_b + (size_t)s * SITE_ELEMS;
+      for (int e = tid; e < CHI * CHI; e += EVOLVE_THREADS) {
+        const int l = e >> 4, r = e & 15;
+        cplx a0 = a[(l * 2 + 0) * CHI + r], a1 = a[(l * 2 + 1) * CHI + r];
+        a[(l * 2 + 0) * CHI + r] = cadd(cmul(u0, a0), cmul(u1, a1));
+        a[(l * 2 + 1) * CHI + r] = cadd(cmul(u2, a0), cmul(u3, a1));
+      }
+    }
+  }
+  for (int s = tid; s <= n; s += EVOLVE_THREADS) p.bonds[(size_t)b * (n + 1) + s] = BOND[s];
+  if (tid == 0) p.status[b] = status;
+}
+
+}  // namespace vqemps

@@ -1,0 +1,282 @@
+// Pauli-sum expectations by shared-prefix left sweeps.
+//
+// Reference algorithm (test/backend/source):
+//   expectPauliShared ......... sharded_mps.cuh:614-687 (sorted words, prefix trie)
+//   analyticLeft/Right/Gather . analytic_batch.cuh:4-36  (E' = A^H P E A per node)
+//   k_rightStage/k_rightFinish  sharded_mps.cuh:61-90    (identity right environments)
+// and the same contraction in test/tools/reverse_mps.py:59-82 (energy_chunk).
+//
+// B200 design. The trie is built once per Hamiltonian over ALL terms (the
+// reference chunks it into <= 128-term pieces and re-uploads it per call) and
+// every path stops at its term's last non-identity site: there the value is
+// closed against the identity right environment R_{s+1} of the state, which is
+// computed once per state. Work is level-synchronous (one launch per site) and
+// batched over B parameter sets. A warp owns one trie parent: it computes
+// S_i = E_parent A_i once for all of its children, then one product per Pauli
+// class present among the children: {I, Z} share t_i = A_i^H S_i
+// (I = t_0 + t_1, Z = t_0 - t_1) and {X, Y} share u_01 = A_0^H S_1 and
+// u_10 = A_1^H S_0 (X = u_01 + u_10, Y = -i u_01 + i u_10). The site tile is
+// staged once per CTA in shared memory; environments are FP64 16 x 16.
+#pragma once
+#include "common.cuh"
+
+namespace vqemps {
+
+struct DevGroup {   // one trie parent with its children at the current level
+  int32_t parent_slot;   // env slot of the parent in the previous level (-1: root)
+  int32_t child_begin;   // first child node (index within the level)
+  int32_t nchild;
+  int32_t classes;       // bit 0: an I or Z child, bit 1: an X or Y child
+};
+
+struct DevNode {    // one trie node
+  int32_t code;          // 0 I, 1 X, 2 Y, 3 Z
+  int32_t env_slot;      // slot in this level's env buffer, -1 if no descendants
+  int32_t leaf;          // leaf id if a term ends here, else -1
+  int32_t pad;
+};
+
+// ---------------------------------------------------------------------------
+// Identity right environments: R_n = 1,
+// R_s[b,b'] = sum_{i,c,c'} conj(A_s[b,i,c]) R_{s+1}[c,c'] A_s[b',i,c'].
+// One CTA per state; R stored for s = 0..n (n+1 tiles of 16x16). When branch is
+// non-null the two physical-index parts M_0, M_1 of every R_s are stored too
+// (the sampler's branch probabilities).
+// ---------------------------------------------------------------------------
+constexpr int RIGHT_THREADS = 256;
+
+__global__ void __launch_bounds__(RIGHT_THREADS)
+right_env_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right,
+                 cplx *__restrict__ branch, const int32_t *__restrict__ status,
+                 double *__restrict__ leafval, int nleaf_total, int identity_leaf) {
+  __shared__ cplx A[SITE_ELEMS];
+  __shared__ cplx R[ENV_ELEMS];
+  __shared__ cplx T[2 * ENV_ELEMS];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const cplx *sb = sites + (size_t)b * n * SITE_ELEMS;
+  cplx *rb = right + (size_t)b * (n + 1) * ENV_ELEMS;
+  R[tid] = cmake(tid == 0 ? 1.0 : 0.0, 0.0);
+  rb[(size_t)n * ENV_ELEMS + tid] = R[tid];
+  for (int s = n - 1; s >= 0; --s) {
+    A[tid] = sb[(size_t)s * SITE_ELEMS + tid];
+    A[tid + 256] = sb[(size_t)s * SITE_ELEMS + tid + 256];
+    __syncthreads();
+    // T_i[c, b'] = sum_c' R[c,c'] A[b',i,c']
+    {
+      const int c = tid >> 4, bp = tid & 15;
+      cplx t0 = cmake(0, 0), t1 = cmake(0, 0);
+      for (int cp = 0; cp < CHI; ++cp) {
+        const cplx r = R[c * CHI + cp];
+        cfma(t0, r, A[(bp * 2 + 0) * CHI + cp]);
+        cfma(t1, r, A[(bp * 2 + 1) * CHI + cp]);
+      }
+      T[c * CHI + bp] = t0;
+      T[ENV_ELEMS + c * CHI + bp] = t1;
+    }
+    __syncthreads();
+    // R_s[bb, b'] = sum_i M_i[bb, b'],  M_i[bb, b'] = sum_c conj(A[bb,i,c]) T_i[c,b']
+    {
+      const int bb = tid >> 4, bp = tid & 15;
+      cplx m0 = cmake(0, 0), m1 = cmake(0, 0);
+      for (int c = 0; c < CHI; ++c) {
+        cfma_conj(m0, A[(bb * 2 + 0) * CHI + c], T[c * CHI + bp]);
+        cfma_conj(m1, A[(bb * 2 + 1) * CHI + c], T[ENV_ELEMS + c * CHI + bp]);
+      }
+      const cplx acc = cadd(m0, m1);
+      R[tid] = acc;
+      rb[(size_t)s * ENV_ELEMS + tid] = acc;
+      if (branch != nullptr) {
+        cplx *mb = branch + ((size_t)b * n + s) * 2 * ENV_ELEMS;
+        mb[tid] = m0;
+        mb[ENV_ELEMS + tid] = m1;
+      }
+    }
+    __syncthreads();
+  }
+  if (identity_leaf >= 0 && tid == 0)
+    leafval[(size_t)b * nleaf_total + identity_leaf] = status[b] == 0 ? R[0].x : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// One trie level for B states.
+// ---------------------------------------------------------------------------
+constexpr int LEVEL_WARPS = 4;
+
+struct LevelParams {
+  const cplx *sites;        // B x n x SITE_ELEMS
+  const cplx *right;        // B x (n+1) x ENV_ELEMS
+  const cplx *env_prev;     // B x nslot_prev x ENV_ELEMS (unused at s = 0)
+  cplx *env_cur;            // B x nslot_cur x ENV_ELEMS
+  const DevGroup *groups;   // this level's groups
+  const DevNode *nodes;     // this level's nodes
+  double *leafval;          // B x nleaf_total
+  int ngroups, nslot_prev, nslot_cur, nleaf_total;
+  int n, s;
+};
+
+struct LevelSmem {
+  cplx A[SITE_ELEMS];
+  cplx E[LEVEL_WARPS][ENV_ELEMS];
+  cplx S[LEVEL_WARPS][2 * ENV_ELEMS];
+};
+
+__global__ void __launch_bounds__(LEVEL_WARPS * 32)
+level_kernel(LevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LevelSmem &sm = *reinterpret_cast<LevelSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+  for (int e = threadIdx.x; e < SITE_ELEMS; e += LEVEL_WARPS * 32) sm.A[e] = ag[e];
+  __syncthreads();
+  const int gidx = blockIdx.x * LEVEL_WARPS + warp;
+  if (gidx >= p.ngroups) return;
+  const DevGroup grp = p.groups[gidx];
+  cplx *E = sm.E[warp];
+  cplx *S = sm.S[warp];
+  const cplx *A = sm.A;
+
+  // parent environment
+  if (grp.parent_slot < 0) {
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
+  } else {
+    const cplx *src = p.env_prev + ((size_t)b * p.nslot_prev + grp.parent_slot) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = src[e];
+  }
+  __syncwarp();
+
+  // ---- S_i[a, c] = sum_a' E[a, a'] A[a', i, c]; lane tile 4 rows x 4 of the 32 columns (i, c)
+  {
+    const int rt = lane >> 3, ct = lane & 7;
+    cplx acc[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[r][c] = cmake(0, 0);
+#pragma unroll 4
+    for (int k = 0; k < CHI; ++k) {
+      cplx e[4], a[4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) e[r] = E[(rt * 4 + r) * CHI + k];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) a[c] = A[k * 2 * CHI + ct * 4 + c];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) cfma(acc[r][c], e[r], a[c]);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int col = ct * 4 + c;          // = i * 16 + c'
+        const int i = col >> 4, cc = col & 15;
+        S[i * ENV_ELEMS + (rt * 4 + r) * CHI + cc] = acc[r][c];
+      }
+  }
+  __syncwarp();
+
+  // ---- second half; lane tile rows 4*rb.. (bra index), columns 2*cb.. (ket index)
+  const int rb = lane >> 3, cb = lane & 7;
+  const cplx *R = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+  for (int cls = 0; cls < 2; ++cls) {
+    if (!(grp.classes & (1 << cls))) continue;
+    cplx t0[4][2], t1[4][2];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+      for (int c = 0; c < 2; ++c) { t0[r][c] = cmake(0, 0); t1[r][c] = cmake(0, 0); }
+    // cls 0: t_i = A_i^H S_i ; cls 1: t0 = A_0^H S_1 (u01), t1 = A_1^H S_0 (u10)
+    const int s0 = cls == 0 ? 0 : 1;
+    const int s1 = cls == 0 ? 1 : 0;
+#pragma unroll 2
+    for (int a = 0; a < CHI; ++a) {
+      cplx av0[4], av1[4], sv0[2], sv1[2];
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        av0[r] = A[(a * 2 + 0) * CHI + rb * 4 + r];
+        av1[r] = A[(a * 2 + 1) * CHI + rb * 4 + r];
+      }
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        sv0[c] = S[s0 * ENV_ELEMS + a * CHI + cb * 2 + c];
+        sv1[c] = S[s1 * ENV_ELEMS + a * CHI + cb * 2 + c];
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          cfma_conj(t0[r][c], av0[r], sv0[c]);
+          cfma_conj(t1[r][c], av1[r], sv1[c]);
+        }
+    }
+    for (int ci = 0; ci < grp.nchild; ++ci) {
+      const DevNode node = p.nodes[grp.child_begin + ci];
+      const bool iz = (node.code == 0 || node.code == 3);
+      if (iz != (cls == 0)) continue;
+      cplx out[4][2];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          if (node.code == 0) out[r][c] = cadd(t0[r][c], t1[r][c]);
+          else if (node.code == 3) out[r][c] = csub(t0[r][c], t1[r][c]);
+          else if (node.code == 1) out[r][c] = cadd(t0[r][c], t1[r][c]);
+          else {  // Y: -i u01 + i u10
+            const cplx d = csub(t1[r][c], t0[r][c]);
+            out[r][c] = cmake(-d.y, d.x);
+          }
+        }
+      if (node.env_slot >= 0) {
+        cplx *dst = p.env_cur + ((size_t)b * p.nslot_cur + node.env_slot) * ENV_ELEMS;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) dst[(rb * 4 + r) * CHI + cb * 2 + c] = out[r][c];
+      }
+      if (node.leaf >= 0) {
+        double v = 0.0;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const cplx rv = R[(rb * 4 + r) * CHI + cb * 2 + c];
+            v += out[r][c].x * rv.x - out[r][c].y * rv.y;
+          }
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) p.leafval[(size_t)b * p.nleaf_total + node.leaf] = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// energies[b] = sum_leaf coef[leaf] * value[b, leaf] (fixed-order tree sum),
+// per_term[b, t] = value[b, term_leaf[t]]. Failed states give NaN.
+// ---------------------------------------------------------------------------
+constexpr int REDUCE_THREADS = 256;
+
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_kernel(const double *__restrict__ leafval, const double *__restrict__ coef, int nleaf,
+              const int32_t *__restrict__ term_leaf, int T, const int32_t *__restrict__ status,
+              double *__restrict__ energies, double *__restrict__ per_term) {
+  __shared__ double part[REDUCE_THREADS];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const double *lv = leafval + (size_t)b * nleaf;
+  const bool ok = status[b] == 0;
+  double acc = 0.0;
+  for (int i = tid; i < nleaf; i += REDUCE_THREADS) acc = fma(coef[i], lv[i], acc);
+  part[tid] = acc;
+  __syncthreads();
+  for (int w = REDUCE_THREADS / 2; w > 0; w >>= 1) {
+    if (tid < w) part[tid] += part[tid + w];
+    __syncthreads();
+  }
+  if (tid == 0) energies[b] = ok ? part[0] : __longlong_as_double(0x7ff8000000000000LL);
+  if (per_term != nullptr) {
+    for (int t = tid; t < T; t += REDUCE_THREADS)
+      per_term[(size_t)b * T + t] = ok ? lv[term_leaf[t]] : __longlong_as_double(0x7ff8000000000000LL);
+  }
+}
+
+}  // namespace vqemps

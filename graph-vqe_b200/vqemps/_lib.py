@@ -1,0 +1,93 @@
+"""ctypes binding of the engine's C ABI (include/vqemps.h).
+
+The shared library is built in-tree (``graph-vqe_b200/vqemps/libvqemps.so``) by
+``vqemps.build``; there is no fallback implementation: every entry point raises
+if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+LIB_NAME = "libvqemps.so"
+LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
+
+OK, INSUFFICIENT_BOND, NONFINITE_SVD, INVALID, CUDA_ERROR, TIMEOUT = range(6)
+
+GATES = dict(rx=0, ry=1, rz=2, h=3, x=4, y=5, z=6, s=7, sdg=8, cx=9, u1=10, u2=11, swap=12)
+INITIAL = {None: 0, "0": 0, "1": 1, "+": 2, "-": 3}
+RNG = dict(splitmix=0, philox=1)
+SHOT_MODES = dict(shared=0, plugin=1)
+
+# Exported symbols of include/vqemps.h (checked by the CPU test suite).
+SYMBOLS = (
+    "vqemps_create", "vqemps_destroy", "vqemps_last_error", "vqemps_set_circuit",
+    "vqemps_num_params", "vqemps_bond_dims", "vqemps_set_hamiltonian",
+    "vqemps_free_hamiltonian", "vqemps_energy_batch", "vqemps_energy_batch_host",
+    "vqemps_batch_status", "vqemps_energy_grad_batch", "vqemps_sample",
+    "vqemps_sampled_energy", "vqemps_copy_sites", "vqemps_plan_stats", "vqemps_profile_energy",
+)
+
+
+class VqempsOp(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("q0", ctypes.c_int32), ("q1", ctypes.c_int32),
+                ("param", ctypes.c_int32), ("angle", ctypes.c_double),
+                ("matrix", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class EngineError(RuntimeError):
+    """A failing engine call; ``code`` is the vqemps_status value."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load the engine library once; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("VQEMPS_LIBRARY", LIB_PATH))
+    if not path.exists():
+        raise ImportError(f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`")
+    lib = ctypes.CDLL(str(path))
+    P, I, D, V = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+    u64 = ctypes.c_uint64
+    sig = {
+        "vqemps_create": (I, [I, I, D, D, ctypes.POINTER(P)]),
+        "vqemps_destroy": (I, [P]),
+        "vqemps_last_error": (ctypes.c_char_p, [P]),
+        "vqemps_set_circuit": (I, [P, I, ctypes.POINTER(VqempsOp), I, ctypes.POINTER(D), I, I, I]),
+        "vqemps_num_params": (I, [P, ctypes.POINTER(I)]),
+        "vqemps_bond_dims": (I, [P, ctypes.POINTER(I)]),
+        "vqemps_set_hamiltonian": (I, [P, ctypes.c_char_p, ctypes.POINTER(D), I, ctypes.POINTER(I)]),
+        "vqemps_free_hamiltonian": (I, [P, I]),
+        "vqemps_energy_batch": (I, [P, I, V, I, V, V, V]),
+        "vqemps_energy_batch_host": (I, [P, I, V, I, V, V, V]),
+        "vqemps_batch_status": (I, [P, ctypes.POINTER(ctypes.c_int32), I, V]),
+        "vqemps_energy_grad_batch": (I, [P, I, V, I, V, V, V]),
+        "vqemps_sample": (I, [P, V, I, I, u64, I, V, V]),
+        "vqemps_sampled_energy": (I, [P, I, V, I, I, u64, I, I, V, V, V]),
+        "vqemps_copy_sites": (I, [P, I, ctypes.POINTER(D), V]),
+        "vqemps_plan_stats": (I, [P, I, ctypes.POINTER(D)]),
+        "vqemps_profile_energy": (I, [P, I, V, I, ctypes.POINTER(D), ctypes.POINTER(I), V]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(ctx, code: int, what: str):
+    """Raise EngineError with the engine's message for a nonzero status."""
+    if code == OK:
+        return
+    msg = load().vqemps_last_error(ctx).decode() if ctx else "invalid call"
+    raise EngineError(code, f"{what}: {msg or 'status ' + str(code)}")

@@ -1,0 +1,270 @@
+"""Python host side of the B200 MPS engine: torch tensors in, torch tensors out.
+
+``Engine`` owns one C-ABI context (one CUDA device). It replaces, for the VQE
+hot path, the state of the reference's NVQIR plugin ``SimulatorMPSDist``
+(test/backend/source/simulator_mps_dist.cu) and its per-thread workspaces.
+Failures raise ``EngineError`` with the reference's messages (insufficient bond,
+nonfinite SVD, invalid Pauli, unsupported gate).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import EngineError, VqempsOp, check, load
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+@dataclass
+class Hamiltonian:
+    """A Pauli sum loaded into an engine (words indexed by qubit)."""
+    handle: int
+    n: int
+    T: int
+    words: list
+    coeffs: np.ndarray
+
+
+def compile_ops(ops, n):
+    """Translate an op list into the C-ABI op array and matrix table.
+
+    Accepted ops (the ``register``/``ReverseMPS`` spec form, reverse_mps.py:12-25,
+    plus the plugin's constant gates and matrices):
+      (gate, q, index)  gate in rx/ry/rz, angle = theta[index]
+      (gate, q, index, scale)  angle = scale * theta[index]
+      (gate, q, None, angle)   constant rotation
+      ('h'|'x'|'y'|'z'|'s'|'sdg', q)
+      ('cx', control, target), ('swap', a, b)
+      ('u1', q, 2x2 matrix), ('u2', q0, q1, 4x4 matrix)
+    """
+    out = []
+    mats = []
+    for op in ops:
+        g = op[0].lower()
+        o = VqempsOp()
+        o.q1 = -1
+        o.param = -1
+        o.angle = 0.0
+        o.matrix = -1
+        if g in ("rx", "ry", "rz"):
+            o.kind = _lib.GATES[g]
+            o.q0 = int(op[1])
+            if len(op) >= 3 and op[2] is not None:
+                o.param = int(op[2])
+                o.angle = float(op[3]) if len(op) > 3 else 1.0
+            else:
+                o.angle = float(op[3])
+        elif g in ("h", "x", "y", "z", "s", "sdg"):
+            o.kind = _lib.GATES[g]
+            o.q0 = int(op[1])
+        elif g in ("cx", "swap"):
+            o.kind = _lib.GATES[g]
+            o.q0, o.q1 = int(op[1]), int(op[2])
+        elif g == "u1":
+            o.kind = _lib.GATES[g]
+            o.q0 = int(op[1])
+            o.matrix = len(mats)
+            mats.extend(np.asarray(op[2], dtype=complex).reshape(4))
+        elif g == "u2":
+            o.kind = _lib.GATES[g]
+            o.q0, o.q1 = int(op[1]), int(op[2])
+            o.matrix = len(mats)
+            mats.extend(np.asarray(op[3], dtype=complex).reshape(16))
+        else:
+            raise EngineError(_lib.INVALID, f"unsupported gate {op[0]!r}")
+        out.append(o)
+    arr = (VqempsOp * max(len(out), 1))(*out)
+    m = np.zeros(2 * max(len(mats), 1))
+    if mats:
+        z = np.asarray(mats, dtype=complex)
+        m[0::2][:len(z)] = z.real
+        m[1::2][:len(z)] = z.imag
+    return arr, len(out), m, len(mats)
+
+
+class Engine:
+    """One engine context on one CUDA device.
+
+    ``site_order='msb'`` maps qubit q to MPS site n-1-q like the plugin
+    (simulator_mps_dist.cu:387); ``'qubit'`` maps it to site q like ReverseMPS.
+    Energies do not depend on the choice; SplitMix sampling reproduces the
+    plugin's shots only with ``'msb'``.
+    """
+
+    def __init__(self, device: int = 0, max_bond: int = 16, abs_cut: float = 0.0,
+                 rel_cut: float = 0.0):
+        self.lib = load()
+        self.device = torch.device("cuda", device)
+        ctx = ctypes.c_void_p()
+        code = self.lib.vqemps_create(device, max_bond, abs_cut, rel_cut, ctypes.byref(ctx))
+        if code != _lib.OK:
+            raise EngineError(code, f"vqemps_create(device={device}, max_bond={max_bond}) failed")
+        self.ctx = ctx
+        self.max_bond = max_bond
+        self.n = 0
+        self.P = 0
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.vqemps_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- circuit / Hamiltonian -------------------------------------------
+    def set_circuit(self, n: int, ops, initial=None, site_order: str = "msb"):
+        arr, count, mats, nm = compile_ops(ops, n)
+        order = {"qubit": 0, "msb": 1}[site_order]
+        mp = mats.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        check(self.ctx, self.lib.vqemps_set_circuit(self.ctx, n, arr, count, mp, nm,
+                                                    _lib.INITIAL[initial], order), "set_circuit")
+        p = ctypes.c_int()
+        check(self.ctx, self.lib.vqemps_num_params(self.ctx, ctypes.byref(p)), "num_params")
+        self.n = n
+        self.P = p.value
+        self.site_order = site_order
+
+    def set_spec(self, spec, site_order: str = "msb"):
+        """Load a ReverseMPS-style spec dict ``{n, ops, initial, count}``."""
+        self.set_circuit(spec["n"], spec["ops"], spec.get("initial"), site_order)
+        self.P = max(self.P, int(spec.get("count", self.P)))
+
+    def bond_dims(self):
+        dims = (ctypes.c_int * (self.n + 1))()
+        check(self.ctx, self.lib.vqemps_bond_dims(self.ctx, dims), "bond_dims")
+        return list(dims)
+
+    def set_hamiltonian(self, words, coeffs) -> Hamiltonian:
+        words = list(words)
+        coeffs = np.ascontiguousarray(coeffs, dtype=np.float64)
+        if len(words) != len(coeffs):
+            raise EngineError(_lib.INVALID, "words and coefficients differ in length")
+        for w in words:
+            if len(w) != self.n:
+                raise EngineError(_lib.INVALID, "Invalid analytic Pauli width")
+        buf = "".join(words).encode("ascii")
+        h = ctypes.c_int()
+        check(self.ctx, self.lib.vqemps_set_hamiltonian(
+            self.ctx, buf, coeffs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+            len(words), ctypes.byref(h)), "set_hamiltonian")
+        return Hamiltonian(h.value, self.n, len(words), words, coeffs)
+
+    def plan_stats(self, ham: Hamiltonian) -> dict:
+        out = (ctypes.c_double * 6)()
+        check(self.ctx, self.lib.vqemps_plan_stats(self.ctx, ham.handle, out), "plan_stats")
+        keys = ("flops", "flops_survey", "node_sites", "groups", "leaves", "max_slots")
+        return dict(zip(keys, list(out)))
+
+    # -- helpers -------------------------------------------------------------
+    def _theta(self, theta):
+        t = torch.as_tensor(theta, dtype=torch.float64, device=self.device)
+        if t.dim() == 1:
+            t = t.unsqueeze(0)
+        if t.shape[1] != self.P:
+            raise EngineError(_lib.INVALID, f"expected {self.P} parameters, got {t.shape[1]}")
+        return t.contiguous()
+
+    def check_status(self, B: int, stream=None):
+        st = (ctypes.c_int32 * B)()
+        code = self.lib.vqemps_batch_status(self.ctx, st, B, _stream(stream))
+        check(self.ctx, code, "batch")
+        return list(st)
+
+    # -- analytic energies ---------------------------------------------------
+    def energy(self, ham: Hamiltonian, theta, per_term: bool = False, stream=None,
+               check_status: bool = True):
+        """Energies of B parameter sets (device tensors); optionally <P_k> per term."""
+        t = self._theta(theta)
+        B = t.shape[0]
+        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        pt = torch.empty((B, ham.T), dtype=torch.float64, device=self.device) if per_term else None
+        check(self.ctx, self.lib.vqemps_energy_batch(self.ctx, ham.handle, _ptr(t), B, _ptr(e), _ptr(pt),
+                                                     _stream(stream)), "energy_batch")
+        if check_status:
+            self.check_status(B, stream)
+        return (e, pt) if per_term else e
+
+    def energy_host(self, ham: Hamiltonian, theta_host: torch.Tensor, out_host: torch.Tensor,
+                    stream=None):
+        """Energies with HOST buffers (pinned CPU tensors): copies inside the call."""
+        B = theta_host.shape[0]
+        check(self.ctx, self.lib.vqemps_energy_batch_host(self.ctx, ham.handle, _ptr(theta_host), B,
+                                                          _ptr(out_host), None, _stream(stream)),
+              "energy_batch_host")
+        return out_host
+
+    def energy_grad(self, ham: Hamiltonian, theta, stream=None):
+        """Energies and dE/dtheta through the exact bond-doubling MPS."""
+        t = self._theta(theta)
+        B = t.shape[0]
+        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        g = torch.empty((B, self.P), dtype=torch.float64, device=self.device)
+        check(self.ctx, self.lib.vqemps_energy_grad_batch(self.ctx, ham.handle, _ptr(t), B, _ptr(e),
+                                                          _ptr(g), _stream(stream)), "energy_grad_batch")
+        return e, g
+
+    # -- sampling ------------------------------------------------------------
+    def sample(self, theta, shots: int, seed: int, rng: str = "splitmix", stream=None):
+        """Packed bitstrings [B, shots, W] (int64 words, bit q = qubit q)."""
+        t = self._theta(theta)
+        B = t.shape[0]
+        W = (self.n + 63) // 64
+        bits = torch.empty((B, shots, W), dtype=torch.int64, device=self.device)
+        check(self.ctx, self.lib.vqemps_sample(self.ctx, _ptr(t), B, shots, seed, _lib.RNG[rng], _ptr(bits),
+                                               _stream(stream)), "sample")
+        self.check_status(B, stream)
+        return bits
+
+    def sampled_energy(self, ham: Hamiltonian, theta, shots: int, seed: int, rng: str = "splitmix",
+                       mode: str = "shared", per_term: bool = False, stream=None):
+        t = self._theta(theta)
+        B = t.shape[0]
+        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        pt = torch.empty((B, ham.T), dtype=torch.float64, device=self.device) if per_term else None
+        check(self.ctx, self.lib.vqemps_sampled_energy(self.ctx, ham.handle, _ptr(t), B, shots, seed,
+                                                       _lib.RNG[rng], _lib.SHOT_MODES[mode], _ptr(e),
+                                                       _ptr(pt), _stream(stream)), "sampled_energy")
+        self.check_status(B, stream)
+        return (e, pt) if per_term else e
+
+    def sites(self, b: int = 0, stream=None) -> np.ndarray:
+        """Padded site tensors [n, 16, 2, 16] of state b of the last batch."""
+        out = np.zeros(self.n * 1024, dtype=np.float64)
+        check(self.ctx, self.lib.vqemps_copy_sites(self.ctx, b, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                                   _stream(stream)), "copy_sites")
+        z = out[0::2] + 1j * out[1::2]
+        return z.reshape(self.n, 16, 2, 16)
+
+
+def unpack_bits(bits: torch.Tensor, n: int) -> np.ndarray:
+    """[B, shots, W] packed words -> uint8 array [B, shots, n] (qubit order)."""
+    b = bits.cpu().numpy().view(np.uint64)
+    q = np.arange(n)
+    words = b[..., q // 64]
+    return ((words >> (q % 64).astype(np.uint64)) & np.uint64(1)).astype(np.uint8)
+
+
+def counts(bits: torch.Tensor, n: int, b: int = 0) -> dict:
+    """CUDA-Q style counts of state b: keys have qubit 0 leftmost (sharded_mps.cuh:896-899)."""
+    arr = unpack_bits(bits[b:b + 1], n)[0]
+    out = {}
+    for row in arr:
+        key = "".join("1" if v else "0" for v in row)
+        out[key] = out.get(key, 0) + 1
+    return out

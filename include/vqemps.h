@@ -1,0 +1,185 @@
+/*
+ * vqemps.h -- C ABI of the B200 matrix-product-state engine for the VQE hot path.
+ *
+ * Plain pointers and sizes only. Device pointers (suffix _dev) are owned by the
+ * caller (for example torch tensors' data_ptr()); the engine owns only its
+ * workspaces. Every call returns a status code (vqemps_status). Calls taking a
+ * stream are stream-ordered and do not synchronise the device, except where a
+ * comment says so.
+ *
+ * Each entry point replaces a part of the reference's CUDA-Q NVQIR plugin
+ * (test/backend/source/simulator_mps_dist.cu, class SimulatorMPSDist) or of its
+ * Python reverse-mode gradient (test/tools/reverse_mps.py); paths are relative to
+ * the hp-cyber/Graph-VQE project root.
+ */
+#ifndef VQEMPS_ABI_H
+#define VQEMPS_ABI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference throws std::runtime_error or calls exit(1):
+ * dist_svd.cuh:22-27 (CUDA/library errors), :277-279 (insufficient bond),
+ * :280-281 (failed or nonfinite SVD), sharded_mps.cuh:643-645 (invalid Pauli),
+ * simulator_mps_dist.cu:235-237,412-415 (too few qubits, unsupported gate). */
+enum vqemps_status {
+  VQEMPS_OK = 0,
+  VQEMPS_INSUFFICIENT_BOND = 1, /* zero-cutoff rank guard fired (reference devInfo rank -2) */
+  VQEMPS_NONFINITE_SVD = 2,     /* nonfinite singular values / no convergence (rank -1)  */
+  VQEMPS_INVALID = 3,           /* bad argument, gate, Pauli character or size           */
+  VQEMPS_CUDA_ERROR = 4,        /* CUDA runtime error                                    */
+  VQEMPS_TIMEOUT = 5            /* a bounded device wait gave up                          */
+};
+
+/* Gate kinds of vqemps_op. Rotations follow CUDA-Q: RX/RY/RZ(t) = exp(-i t P / 2). */
+enum vqemps_gate {
+  VQEMPS_RX = 0, VQEMPS_RY = 1, VQEMPS_RZ = 2,
+  VQEMPS_H = 3, VQEMPS_X = 4, VQEMPS_Y = 5, VQEMPS_Z = 6, VQEMPS_S = 7, VQEMPS_SDG = 8,
+  VQEMPS_CX = 9,    /* q0 = control, q1 = target                                         */
+  VQEMPS_U1 = 10,   /* 2x2 row-major matrix from the matrix table, on q0                 */
+  VQEMPS_U2 = 11,   /* 4x4 row-major [(I*2+J)*4+(i*2+j)] on (q0 -> I, q1 -> J)            */
+  VQEMPS_SWAP = 12
+};
+
+/* Initial product state of every qubit (reverse_mps.py:41-43). */
+enum vqemps_initial { VQEMPS_INIT_ZERO = 0, VQEMPS_INIT_ONE = 1, VQEMPS_INIT_PLUS = 2, VQEMPS_INIT_MINUS = 3 };
+
+/* Random number generator of the sampler. SPLITMIX reproduces the reference's
+ * per-(seed, site, shot) hash draw (sharded_mps.cuh:147-170); PHILOX is
+ * Philox4x32-10 with counter (shot, site, 0, 0) and key (seed lo, seed hi). */
+enum vqemps_rng { VQEMPS_RNG_SPLITMIX = 0, VQEMPS_RNG_PHILOX = 1 };
+
+/* One circuit operation. A GateApplicationTask of the plugin
+ * (simulator_mps_dist.cu:1392-1406) is {name, matrix, controls, targets,
+ * parameters}; here it is {kind, qubits, parameter index or constant angle,
+ * matrix-table index}. */
+typedef struct vqemps_op {
+  int32_t kind;    /* vqemps_gate                                          */
+  int32_t q0;      /* target (1q), control (CX), first qubit (U2, SWAP)    */
+  int32_t q1;      /* target (CX), second qubit (U2, SWAP), else -1        */
+  int32_t param;   /* rotation angle = theta[param] * scale, or -1          */
+  double angle;    /* rotation angle when param < 0; scale when param >= 0 */
+  int32_t matrix;  /* index into the matrix table (U1: 4, U2: 16 complex)  */
+  int32_t pad;
+} vqemps_op;
+
+typedef struct vqemps_ctx vqemps_ctx;
+
+/* Create an engine on a CUDA device. Replaces SimulatorMPSDist::ensureEngine's
+ * configuration (simulator_mps_dist.cu:363-366: CUDAQ_MPS_MAX_BOND /
+ * _ABS_CUTOFF / _RELATIVE_CUTOFF) and the thread-local handle pool
+ * (sharded_mps.cuh:276-305). max_bond <= 16 (the engine's padded bond). */
+int vqemps_create(int device, int max_bond, double abs_cut, double rel_cut, vqemps_ctx **out);
+
+/* Release all device memory of the engine (ShardedMPS::~ShardedMPS,
+ * sharded_mps.cuh:413-427; AnalyticWorkspace::release, analytic_batch.cuh:44-52). */
+int vqemps_destroy(vqemps_ctx *ctx);
+
+/* Message of the last failing call on this context (never NULL). */
+const char *vqemps_last_error(const vqemps_ctx *ctx);
+
+/* Load a circuit: replaces addQubitsToState + the applyGate sequence of one
+ * kernel execution (simulator_mps_dist.cu:1371-1406, 376-416). Qubit q maps to
+ * MPS site q when site_order == 0, and to site n-1-q when site_order == 1 (the
+ * plugin's msb map conv(q) = n-1-q, simulator_mps_dist.cu:387). Non-adjacent
+ * two-qubit gates are routed by SWAPs as in ShardedMPS::applyTwoQubit
+ * (sharded_mps.cuh:565-572). matrices: nmatrices complex numbers as (re, im)
+ * pairs. Returns VQEMPS_INVALID for n < 2 (simulator_mps_dist.cu:235-237) or an
+ * unsupported gate (:412-415). */
+int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, int nops,
+                       const double *matrices, int nmatrices, int initial, int site_order);
+
+/* Number of circuit parameters (largest param index + 1) and bond dimensions
+ * (n + 1 entries) that the zero-cutoff SVD keeps, the allocation bound of
+ * graph_resources.allocation_bound (test/tools/graph_resources.py:12-32). */
+int vqemps_num_params(const vqemps_ctx *ctx, int *params);
+int vqemps_bond_dims(const vqemps_ctx *ctx, int *dims);
+
+/* Load a Pauli sum: words is T rows of n characters over {I,X,Y,Z}, indexed by
+ * QUBIT (row t, column q); coeffs are the real coefficients. The shared-prefix
+ * plan is built and uploaded once per Hamiltonian (the reference rebuilds its
+ * key-cached plan and re-uploads it on every call: sharded_mps.cuh:627-672).
+ * Replaces buildPauliTermData (simulator_mps_dist.cu:571-583). */
+int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const double *coeffs, int T,
+                           int *handle);
+int vqemps_free_hamiltonian(vqemps_ctx *ctx, int handle);
+
+/* Analytic energies of B parameter sets: E[b] = sum_k c_k Re<psi_b|P_k|psi_b>.
+ * Replaces observe() with shots = -1 (simulator_mps_dist.cu:1434-1485) and
+ * expectPauliShared (sharded_mps.cuh:614-687) for B states in one call.
+ * theta_dev: B x P doubles; energies_dev: B doubles; per_term_dev: B x T doubles
+ * of <P_k> (the ExecutionResult per term id, simulator_mps_dist.cu:1467-1481) or
+ * NULL. Stream-ordered; per-state failures are reported by vqemps_batch_status. */
+int vqemps_energy_batch(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,
+                        double *energies_dev, double *per_term_dev, void *stream);
+
+/* Same as vqemps_energy_batch with HOST buffers: copies theta in and energies
+ * (and per_term when non-NULL) out on the stream, then synchronises the stream
+ * and returns the first per-state failure as the status. */
+int vqemps_energy_batch_host(vqemps_ctx *ctx, int handle, const double *theta, int B,
+                             double *energies, double *per_term, void *stream);
+
+/* Per-state status of the last batched call (synchronises the stream). */
+int vqemps_batch_status(vqemps_ctx *ctx, int32_t *status, int B, void *stream);
+
+/* Energy and gradient dE/dtheta of B parameter sets through the exact
+ * bond-doubling MPS (no SVD), the quantity of ReverseMPS.value_gradient
+ * (reverse_mps.py:84-99). grad_dev: B x P doubles. Requires a circuit whose
+ * two-qubit gates are adjacent CX (the ReverseMPS/register restriction,
+ * reverse_mps.py:12-25). */
+int vqemps_energy_grad_batch(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,
+                             double *energies_dev, double *grad_dev, void *stream);
+
+/* Perfect sampling of B states: shots bitstrings each, bit q of shot s of state
+ * b in packed_dev[(b * shots + s) * W + q / 64] >> (q % 64), W = ceil(n / 64),
+ * QUBIT order, n <= 256. Replaces sample() without noise
+ * (simulator_mps_dist.cu:1587-1613) and sampleBitsGpu (sharded_mps.cuh:814-902).
+ * seed is the evaluation seed of state 0 (the plugin's sampleSeed++ value); state
+ * b uses seed + b. With VQEMPS_RNG_SPLITMIX the draw seed is
+ * hbatchSeedForShotShard(seed + b, 0) (simulator_mps_dist.cu:596-608), so with
+ * site_order 1 the shots are the plugin's. */
+int vqemps_sample(vqemps_ctx *ctx, const double *theta_dev, int B, int shots, uint64_t seed,
+                  int rng, uint64_t *packed_dev, void *stream);
+
+/* Shot-estimated energies. Replaces observe() with finite shots
+ * (simulator_mps_dist.cu:1487-1515). Words with X or Y are evaluated
+ * analytically in both modes (evaluateHbatchTermBatch, simulator_mps_dist.cu:661-700).
+ * mode VQEMPS_SHOTS_SHARED: every I/Z word is estimated from one shared sample
+ *   set per state (runSharedDiagonalShotBatch, :1157-1171; sampleZExpectationsGpu,
+ *   sharded_mps.cuh:906-935).
+ * mode VQEMPS_SHOTS_PLUGIN: the plugin's rule -- shared when every word is I/Z,
+ *   otherwise an independent stream per non-identity I/Z word
+ *   (sampleZExpectationsIndependentGpu, sharded_mps.cuh:942-982).
+ * seed is the evaluation seed of state 0 (state b uses seed + b).
+ * per_term_dev (B x T) or NULL. */
+enum vqemps_shot_mode { VQEMPS_SHOTS_SHARED = 0, VQEMPS_SHOTS_PLUGIN = 1 };
+int vqemps_sampled_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int B, int shots,
+                          uint64_t seed, int rng, int mode, double *energies_dev,
+                          double *per_term_dev, void *stream);
+
+/* Benchmark support (no reference counterpart): phase times of one batched
+ * energy call -- ms[0] state preparation, ms[1] right environments, ms[2] trie
+ * levels, ms[3] energy reduction -- and the number of kernels one call launches.
+ * Synchronises the stream. */
+int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int B, double *ms,
+                          int *launches, void *stream);
+
+/* Work statistics of a loaded Pauli sum, per state and evaluation: stats[0]
+ * FP64 flops as executed, stats[1] the survey count 16 Dl Dr (Dl + Dr) per trie
+ * node-site, stats[2] node-sites, stats[3] parent groups, stats[4] leaves,
+ * stats[5] largest environment slot count of a level. */
+int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats);
+
+/* Copy the site tensors of state b of the last batched call to the host:
+ * n * 16 * 2 * 16 complex (re, im) pairs, site s at offset s * 1024 doubles,
+ * element (l, p, r) at ((l * 2 + p) * 16 + r), zero padded beyond the bond dims.
+ * Used to check the prepared state against the oracle (synchronises). */
+int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VQEMPS_ABI_H */
