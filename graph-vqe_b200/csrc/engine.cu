@@ -598,6 +598,7 @@ extern "C" int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stat
 // ---------------------------------------------------------------------------
 static int ensure_state_ws(vqemps_ctx *ctx, int B) {
   const int n = ctx->n;
+  if (B > 65535) return fail(ctx, VQEMPS_INVALID, "at most 65535 parameter sets per call");
   CUDA_TRY(ctx, ctx->sites.ensure((size_t)B * n * SITE_ELEMS));
   CUDA_TRY(ctx, ctx->bonds_ws.ensure((size_t)B * (n + 1)));
   CUDA_TRY(ctx, ctx->status.ensure((size_t)B));
