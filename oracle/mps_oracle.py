@@ -632,7 +632,7 @@ def z_sample_sums(bits, words):
     sums = []
     for w in words:
         mask = np.array([c == "Z" for c in w])
-        parity = bits[:, mask].sum(axis=1) & 1
+        parity = bits[:, mask].astype(np.int64).sum(axis=1) & 1
         sums.append(int(np.sum(1 - 2 * parity)))
     return np.array(sums, dtype=np.int64)
 

@@ -172,3 +172,8 @@ def test_cpu_baseline_matches_reference(case):
     spec = _spec(case)
     e = cpu_baseline.energy(spec, case["words"], np.array(case["coeffs"]), np.array(case["x"]), threads=4)
     assert abs(e - case["energy"]) <= 1e-10 * max(1.0, abs(case["energy"]))
+
+
+def test_z_sample_sums_on_unsigned_bits():
+    bits = np.array([[1, 0, 1], [0, 0, 1]], dtype=np.uint8)
+    assert list(O.z_sample_sums(bits, ["ZZI", "IIZ", "III"])) == [0, -2, 2]
