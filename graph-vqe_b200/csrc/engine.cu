@@ -806,3 +806,4 @@ extern "C" int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, voi
 
 #include "engine_sample.inc"
 #include "engine_grad.inc"
+#include "noalloc.cu"

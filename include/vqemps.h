@@ -179,6 +179,22 @@ int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats);
  * Used to check the prepared state against the oracle (synchronises). */
 int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, void *stream);
 
+/* Allocation-free analytic energy of ONE parameter set. No counterpart in the
+ * reference: it exists for callers that must not allocate device memory while
+ * they run -- for example a simulator plugin hosted inside a runtime that owns
+ * all device memory through its own pool, or an operator under a fixed memory
+ * budget -- because vqemps_energy_batch grows its workspaces with cudaMalloc.
+ * All intermediate data live in one static device array of 22 MiB per GPU,
+ * held until the process exits. Limits: <= 64 qubits, <= 2560 environments kept
+ * on one site, <= 16384 distinct term endings (VQEMPS_INVALID beyond them).
+ * Calls share that array: calls that overlap on the GPU race and must be
+ * serialised by the caller. The first call on a device looks the array up
+ * (make it before any stream capture). theta_dev: P doubles; energy_dev: 1
+ * double (NaN if the state failed); per_term_dev: T doubles or NULL;
+ * status_dev: 1 int32 (vqemps_status of the state) or NULL. */
+int vqemps_energy_noalloc(vqemps_ctx *ctx, int handle, const double *theta_dev, double *energy_dev,
+                          double *per_term_dev, int32_t *status_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
