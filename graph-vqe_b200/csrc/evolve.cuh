@@ -100,7 +100,6 @@ evolve_kernel(EvolveParams p) {
   double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
   int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
   int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
-  double *MISCD = reinterpret_cast<double *>(smem + EvolveSmem::MISC + 16);
   cplx *PEND = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);
   int *BOND = reinterpret_cast<int *>(smem + EvolveSmem::PEND + p.n * 4 * 16);
 
@@ -198,21 +197,35 @@ evolve_kernel(EvolveParams p) {
     __syncthreads();
     double total = 0.0;
     for (int w = 0; w < EVOLVE_THREADS / 32; ++w) total += NORM[w];
-    // Rows below eps * ||Theta||_F are numerically null: pairs whose coupling is
-    // below this floor are left alone, which keeps rank-deficient Theta from
-    // rotating rounding noise forever.
+    // Rows below eps * ||Theta||_F are numerically null: pairs whose coupling
+    // |gamma| is below eps^2 ||Theta||_F^2 are left alone, which keeps a
+    // rank-deficient Theta from rotating rounding noise forever.
     const double floor_g = eps * eps * total;
-    const double tol = 4.0 * eps;
+    const double floor2 = floor_g * floor_g;
+    const double tol2 = 16.0 * eps * eps;        // |gamma| > 4 eps sqrt(alpha beta)
+    __syncthreads();
 
     // ---- one-sided Jacobi on the rows of Theta, round-robin pair ordering ----
+    // A pair (p, q) with alpha = |X_p|^2, beta = |X_q|^2, gamma = X_p . X_q^H is
+    // rotated by J = c [[1, -w gamma], [w conj(gamma), 1]] with
+    // w = 2 sign(d) / (|d| + sqrt(d^2 + 4 |gamma|^2)), d = beta - alpha,
+    // c = 1 / sqrt(1 + w^2 |gamma|^2): the classical Jacobi rotation with the
+    // phase of gamma moved onto row q (V absorbs it). Row norms then move by
+    // -+ w |gamma|^2 and are kept in NORM, recomputed exactly after each sweep.
     const int pair = tid >> 4, lane = tid & 15;
     const int npairs = m >> 1;
-    bool converged = (m == 1);
+    if (tid < m) {
+      double a = 0.0;
+      for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
+      NORM[tid] = a;
+    }
+    __syncthreads();
+    bool converged = false;
     for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
       int rotated = 0;
       for (int step = 0; step < m - 1; ++step) {
         int pr = 0, qr = 0;
-        bool active = pair < npairs;
+        const bool active = pair < npairs;
         if (active) {
           const int mm1 = m - 1;
           if (pair == 0) { pr = 0; qr = 1 + (step % mm1); }
@@ -225,53 +238,53 @@ evolve_kernel(EvolveParams p) {
           if (j0 < ncol) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
           if (j1 < ncol) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
         }
-        double al = cabs2(xp0) + cabs2(xp1);
-        double be = cabs2(xq0) + cabs2(xq1);
         // gamma = sum_j X[p,j] conj(X[q,j])
         double gr = xp0.x * xq0.x + xp0.y * xq0.y + xp1.x * xq1.x + xp1.y * xq1.y;
         double gim = xp0.y * xq0.x - xp0.x * xq0.y + xp1.y * xq1.x - xp1.x * xq1.y;
         for (int o = 8; o > 0; o >>= 1) {
-          al += __shfl_xor_sync(0xffffffffu, al, o, 16);
-          be += __shfl_xor_sync(0xffffffffu, be, o, 16);
           gr += __shfl_xor_sync(0xffffffffu, gr, o, 16);
           gim += __shfl_xor_sync(0xffffffffu, gim, o, 16);
         }
-        const double ag = sqrt(gr * gr + gim * gim);
-        if (active && ag > floor_g && ag > tol * sqrt(al * be)) {
+        const double al = active ? NORM[pr] : 0.0, be = active ? NORM[qr] : 0.0;
+        const double g2 = gr * gr + gim * gim;
+        if (active && g2 > floor2 && g2 > tol2 * al * be) {
           rotated = 1;
-          const double zeta = (be - al) / (2.0 * ag);
-          const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-          const double c = 1.0 / sqrt(1.0 + t * t);
-          const double sn = t * c;
-          const cplx e = cmake(gr / ag, gim / ag);          // e^{i phi}
-          const cplx es = cscale(e, sn), ec = cscale(e, c);
-          // X_p' = c X_p - s e X_q ; X_q' = s X_p + c e X_q
+          const double d = be - al;
+          const double w = copysign(2.0, d) / (fabs(d) + sqrt(d * d + 4.0 * g2));
+          const double c = rsqrt(1.0 + w * w * g2);
+          const cplx wg = cmake(w * gr, w * gim);             // w gamma
+          const cplx wgc = cconj(wg);                         // w conj(gamma)
           if (j0 < ncol) {
-            X[pr * 32 + j0] = csub(cscale(xp0, c), cmul(es, xq0));
-            X[qr * 32 + j0] = cadd(cscale(xp0, sn), cmul(ec, xq0));
+            X[pr * 32 + j0] = cscale(csub(xp0, cmul(wg, xq0)), c);
+            X[qr * 32 + j0] = cscale(cadd(cmul(wgc, xp0), xq0), c);
           }
           if (j1 < ncol) {
-            X[pr * 32 + j1] = csub(cscale(xp1, c), cmul(es, xq1));
-            X[qr * 32 + j1] = cadd(cscale(xp1, sn), cmul(ec, xq1));
+            X[pr * 32 + j1] = cscale(csub(xp1, cmul(wg, xq1)), c);
+            X[qr * 32 + j1] = cscale(cadd(cmul(wgc, xp1), xq1), c);
           }
-          // V[:,p]' = c V_p - s conj(e) V_q ; V[:,q]' = s V_p + c conj(e) V_q
-          const cplx esc = cconj(es), ecc = cconj(ec);
+          // V <- V J^H: V_p' = c (V_p - w conj(gamma) V_q), V_q' = c (w gamma V_p + V_q)
           for (int i = lane; i < m; i += 16) {
-            cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
-            VT[pr * 32 + i] = csub(cscale(vp, c), cmul(esc, vq));
-            VT[qr * 32 + i] = cadd(cscale(vp, sn), cmul(ecc, vq));
+            const cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
+            VT[pr * 32 + i] = cscale(csub(vp, cmul(wgc, vq)), c);
+            VT[qr * 32 + i] = cscale(cadd(cmul(wg, vp), vq), c);
+          }
+          if (lane == 0) {
+            NORM[pr] = al - w * g2;
+            NORM[qr] = be + w * g2;
           }
         }
         __syncthreads();
       }
       converged = !__syncthreads_or(rotated);
+      if (tid < m) {
+        double a = 0.0;
+        for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
+        NORM[tid] = a;
+      }
+      __syncthreads();
     }
     // ---- singular values = row norms, sorted descending (stable in row index) ----
-    if (tid < m) {
-      double a = 0.0;
-      for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
-      NORM[tid] = sqrt(a);
-    }
+    if (tid < m) NORM[tid] = sqrt(NORM[tid]);
     __syncthreads();
     if (tid < m) {
       const double v = NORM[tid];

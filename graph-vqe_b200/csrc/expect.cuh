@@ -116,11 +116,16 @@ struct LevelParams {
 
 struct LevelSmem {
   cplx A[SITE_ELEMS];
-  cplx E[LEVEL_WARPS][ENV_ELEMS];
-  cplx S[LEVEL_WARPS][2 * ENV_ELEMS];
+  cplx W[LEVEL_WARPS][2 * ENV_ELEMS];   // per warp: parent E (first 4 KiB), then S_0 | S_1
 };
 
-__global__ void __launch_bounds__(LEVEL_WARPS * 32)
+// Lane layout (conflict-free shared-memory access): a quarter-warp (8 lanes with
+// equal lane >> 3) always reads 8 consecutive complex numbers of one row
+// (128 bytes) or one broadcast address.
+//   first half:  rows 4*(lane>>3) .. +3 of S, columns (lane&7) + 8c, c = 0..3,
+//                of the 32-column panel [S_0 | S_1]
+//   second half: rows 4*(lane>>3) .. +3 of E', columns (lane&7) + 8c, c = 0..1
+__global__ void __launch_bounds__(LEVEL_WARPS * 32, 4)
 level_kernel(LevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LevelSmem &sm = *reinterpret_cast<LevelSmem *>(smem_raw);
@@ -132,9 +137,10 @@ level_kernel(LevelParams p) {
   const int gidx = blockIdx.x * LEVEL_WARPS + warp;
   if (gidx >= p.ngroups) return;
   const DevGroup grp = p.groups[gidx];
-  cplx *E = sm.E[warp];
-  cplx *S = sm.S[warp];
+  cplx *E = sm.W[warp];
+  cplx *S = sm.W[warp];
   const cplx *A = sm.A;
+  const int rq = lane >> 3, cq = lane & 7;
 
   // parent environment
   if (grp.parent_slot < 0) {
@@ -145,39 +151,35 @@ level_kernel(LevelParams p) {
   }
   __syncwarp();
 
-  // ---- S_i[a, c] = sum_a' E[a, a'] A[a', i, c]; lane tile 4 rows x 4 of the 32 columns (i, c)
+  // ---- S_i[a, c] = sum_a' E[a, a'] A[a', i, c]
   {
-    const int rt = lane >> 3, ct = lane & 7;
     cplx acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
       for (int c = 0; c < 4; ++c) acc[r][c] = cmake(0, 0);
-#pragma unroll 4
+#pragma unroll 2
     for (int k = 0; k < CHI; ++k) {
       cplx e[4], a[4];
 #pragma unroll
-      for (int r = 0; r < 4; ++r) e[r] = E[(rt * 4 + r) * CHI + k];
+      for (int r = 0; r < 4; ++r) e[r] = E[(rq * 4 + r) * CHI + k];
 #pragma unroll
-      for (int c = 0; c < 4; ++c) a[c] = A[k * 2 * CHI + ct * 4 + c];
+      for (int c = 0; c < 4; ++c) a[c] = A[k * 2 * CHI + cq + 8 * c];
 #pragma unroll
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 4; ++c) cfma(acc[r][c], e[r], a[c]);
     }
+    __syncwarp();            // all lanes are done reading E before S overwrites it
 #pragma unroll
     for (int r = 0; r < 4; ++r)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int col = ct * 4 + c;          // = i * 16 + c'
-        const int i = col >> 4, cc = col & 15;
-        S[i * ENV_ELEMS + (rt * 4 + r) * CHI + cc] = acc[r][c];
-      }
+      for (int c = 0; c < 4; ++c)  // panel column cq + 8c = i * 16 + c'
+        S[(c >> 1) * ENV_ELEMS + (rq * 4 + r) * CHI + cq + 8 * (c & 1)] = acc[r][c];
   }
   __syncwarp();
 
-  // ---- second half; lane tile rows 4*rb.. (bra index), columns 2*cb.. (ket index)
-  const int rb = lane >> 3, cb = lane & 7;
+  // ---- second half
   const cplx *R = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
   for (int cls = 0; cls < 2; ++cls) {
     if (!(grp.classes & (1 << cls))) continue;
@@ -191,24 +193,22 @@ level_kernel(LevelParams p) {
     const int s1 = cls == 0 ? 1 : 0;
 #pragma unroll 2
     for (int a = 0; a < CHI; ++a) {
-      cplx av0[4], av1[4], sv0[2], sv1[2];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        av0[r] = A[(a * 2 + 0) * CHI + rb * 4 + r];
-        av1[r] = A[(a * 2 + 1) * CHI + rb * 4 + r];
-      }
+      cplx sv0[2], sv1[2];
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
-        sv0[c] = S[s0 * ENV_ELEMS + a * CHI + cb * 2 + c];
-        sv1[c] = S[s1 * ENV_ELEMS + a * CHI + cb * 2 + c];
+        sv0[c] = S[s0 * ENV_ELEMS + a * CHI + cq + 8 * c];
+        sv1[c] = S[s1 * ENV_ELEMS + a * CHI + cq + 8 * c];
       }
 #pragma unroll
-      for (int r = 0; r < 4; ++r)
+      for (int r = 0; r < 4; ++r) {
+        const cplx av0 = A[(a * 2 + 0) * CHI + rq * 4 + r];
+        const cplx av1 = A[(a * 2 + 1) * CHI + rq * 4 + r];
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-          cfma_conj(t0[r][c], av0[r], sv0[c]);
-          cfma_conj(t1[r][c], av1[r], sv1[c]);
+          cfma_conj(t0[r][c], av0, sv0[c]);
+          cfma_conj(t1[r][c], av1, sv1[c]);
         }
+      }
     }
     for (int ci = 0; ci < grp.nchild; ++ci) {
       const DevNode node = p.nodes[grp.child_begin + ci];
@@ -219,9 +219,8 @@ level_kernel(LevelParams p) {
       for (int r = 0; r < 4; ++r)
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-          if (node.code == 0) out[r][c] = cadd(t0[r][c], t1[r][c]);
+          if (node.code == 0 || node.code == 1) out[r][c] = cadd(t0[r][c], t1[r][c]);
           else if (node.code == 3) out[r][c] = csub(t0[r][c], t1[r][c]);
-          else if (node.code == 1) out[r][c] = cadd(t0[r][c], t1[r][c]);
           else {  // Y: -i u01 + i u10
             const cplx d = csub(t1[r][c], t0[r][c]);
             out[r][c] = cmake(-d.y, d.x);
@@ -232,7 +231,7 @@ level_kernel(LevelParams p) {
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-          for (int c = 0; c < 2; ++c) dst[(rb * 4 + r) * CHI + cb * 2 + c] = out[r][c];
+          for (int c = 0; c < 2; ++c) dst[(rq * 4 + r) * CHI + cq + 8 * c] = out[r][c];
       }
       if (node.leaf >= 0) {
         double v = 0.0;
@@ -240,7 +239,7 @@ level_kernel(LevelParams p) {
         for (int r = 0; r < 4; ++r)
 #pragma unroll
           for (int c = 0; c < 2; ++c) {
-            const cplx rv = R[(rb * 4 + r) * CHI + cb * 2 + c];
+            const cplx rv = R[(rq * 4 + r) * CHI + cq + 8 * c];
             v += out[r][c].x * rv.x - out[r][c].y * rv.y;
           }
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
