@@ -152,25 +152,30 @@ def cpu_reference_rate(seconds, threads):
 
 
 def run_reference(args):
+    """Reference arm: the CPU restatement of the reference's energy path, each step a
+    bounded sample of the workload (a fixed number of parameter sets), all host threads."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import cpu_baseline
     threads = os.cpu_count() or 1
-    per_step = []
-    samples = []
-    for k in range(args.warmup + args.steps):
-        r = cpu_reference_rate(max(2.0, args.cpu_sample_seconds / max(1, args.steps)), threads)
-        if k >= args.warmup:
-            per_step.append(r["value"])
-            samples.append(r)
-    value = float(np.mean(per_step))
+    w = cpu_baseline.Workload(args.batch)
+    dt = w.run(1, threads)                                   # warm-up; sizes a ~2 s step
+    per_step = max(1, int(round(2.0 / max(dt, 1e-3))))
+    for _ in range(args.warmup):
+        w.run(per_step, threads)
+    total = 0.0
+    for _ in range(args.steps):
+        total += w.run(per_step, threads)
+    evals = per_step * args.steps
+    value = evals / total
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=args.gpus, steps=args.steps, warmup=args.warmup,
-                ms_per_step=1000.0 * samples[0]["seconds"] / max(samples[0]["evals"], 1),
-                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="c128", data="synthetic",
-                impl="reference",
-                config=dict(WORKLOAD, global_batch=args.batch, parallelism="host threads"),
+                ms_per_step=1000.0 * total / args.steps, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="c128", data="synthetic", impl="reference",
+                config=dict(WORKLOAD, global_batch=args.batch, parallelism=f"{threads} host threads",
+                            evals_per_step=per_step),
                 cpu_baseline=dict(value=value, unit=UNIT, cores=threads, kind="port",
-                                  sample=samples[0]["sample"]),
+                                  sample=cpu_baseline.describe(evals, total, threads)),
                 e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line))
 
