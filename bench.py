@@ -239,9 +239,13 @@ def main():
     level_s = phases["levels_s"]
     flops_step = stats["flops"] * args.batch
     achieved = flops_step / level_s / 1e12
-    roofline = dict(bound="fp64", achieved=achieved, peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
-                    traffic=None, kernel="level_kernel (all trie levels of one step)",
-                    peak_source="cuBLAS FP64 DGEMM 8192^3 measured in this run (burst)",
+    variant = eng.level_variant(ham, args.batch)
+    kernel = {"simt": "level_kernel (FP64 FMA pipes)", "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
+              "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)"}.get(variant, str(variant))
+    roofline = dict(bound="tensor" if variant and variant.startswith("dmma") else "fp64", achieved=achieved,
+                    peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak, traffic=None,
+                    kernel=kernel + ", all trie levels of one step",
+                    peak_source="cuBLAS FP64 DGEMM 8192^3 (DMMA tensor cores) measured in this run, burst",
                     survey_unit_tflops=stats["flops_survey"] * args.batch / level_s / 1e12)
 
     # ---- e2e: host buffers through the C ABI, copies inside the timed region ----

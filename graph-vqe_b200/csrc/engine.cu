@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "evolve.cuh"
 #include "expect.cuh"
+#include "expect_mma.cuh"
 #include "sample.cuh"
 #include "gradient.cuh"
 
@@ -36,6 +37,7 @@ struct Hamiltonian {
   std::vector<DevNode> nodes;
   std::vector<int32_t> leaf_level;       // level of every leaf (-1: identity)
   int max_slot = 1;
+  std::map<int, int> tuned;              // batch-size bucket -> level kernel variant
   // work accounting (FP64 real flops of one evaluation of one state)
   double flops = 0.0;
   double flops_survey = 0.0;
@@ -118,6 +120,7 @@ struct vqemps_ctx {
   DevBuf<cplx> grad_sites, grad_envs, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
   DevBuf<double> grad_stage;
   int last_B = 0;
+  int forced_variant = -1;              // level kernel variant, -1: autotune
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
@@ -161,6 +164,14 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(evolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelSmem));
+  cudaFuncSetAttribute(level_mma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelMmaSmem<4>));
+  cudaFuncSetAttribute(level_mma_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelMmaSmem<8>));
+  cudaFuncSetAttribute(level_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelPfSmem));
+  cudaFuncSetAttribute(level_mma_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelMmaPfSmem));
   grad_set_attributes();
   *out = ctx;
   return VQEMPS_OK;
@@ -639,14 +650,39 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
   return VQEMPS_OK;
 }
 
-// Trie levels and the energy reduction on the prepared states (needs launch_right first).
-static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
-                         double *energies_dev, double *per_term_dev) {
+// Level kernel variants: the autotuner times each on the caller's workload.
+enum : int { LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_COUNT = 5 };
+
+static void launch_level_variant(int variant, const LevelParams &lp, int ng, int B, cudaStream_t st) {
+  switch (variant) {
+    case LV_MMA4:
+      level_mma_kernel<4><<<dim3((ng + 3) / 4, B), 4 * 32, sizeof(LevelMmaSmem<4>), st>>>(lp);
+      break;
+    case LV_MMA8:
+      level_mma_kernel<8><<<dim3((ng + 7) / 8, B), 8 * 32, sizeof(LevelMmaSmem<8>), st>>>(lp);
+      break;
+    case LV_PF4: {
+      // about four parents per warp, never fewer than one CTA per state
+      const int gpw = ng >= 4 * PF_WARPS ? 4 : 1;
+      const int ctas = (ng + PF_WARPS * gpw - 1) / (PF_WARPS * gpw);
+      level_pf_kernel<<<dim3(ctas, B), PF_WARPS * 32, sizeof(LevelPfSmem), st>>>(lp, gpw);
+      break;
+    }
+    case LV_MMAPF4: {
+      const int gpw = ng >= 4 * MPF_WARPS ? 4 : 1;
+      const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
+      level_mma_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
+      break;
+    }
+    default:
+      level_kernel<<<dim3((ng + LEVEL_WARPS - 1) / LEVEL_WARPS, B), LEVEL_WARPS * 32, sizeof(LevelSmem), st>>>(lp);
+  }
+}
+
+// All trie levels of one evaluation with a given variant (needs launch_right first).
+static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int variant) {
   const int n = ctx->n;
   const int nleaf = std::max(h.nleaf, 1);
-  CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
-  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * h.max_slot * ENV_ELEMS));
-  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * h.max_slot * ENV_ELEMS));
   cplx *envs[2] = {ctx->env0.ptr, ctx->env1.ptr};
   for (int s = 0; s < n; ++s) {
     const int ng = h.group_off[s + 1] - h.group_off[s];
@@ -665,10 +701,62 @@ static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st
     lp.nleaf_total = nleaf;
     lp.n = n;
     lp.s = s;
-    dim3 grid((ng + LEVEL_WARPS - 1) / LEVEL_WARPS, B);
-    level_kernel<<<grid, LEVEL_WARPS * 32, sizeof(LevelSmem), st>>>(lp);
+    launch_level_variant(variant, lp, ng, B, st);
     CUDA_TRY(ctx, cudaGetLastError());
   }
+  return VQEMPS_OK;
+}
+
+static int batch_bucket(int B) {
+  int k = 0;
+  while ((1 << k) < B) ++k;
+  return k;
+}
+
+// Variant for (plan, batch size): forced, cached, or measured now. Tuning
+// times every variant once on the prepared states (CUDA events, synchronising
+// the stream once per plan and batch-size bucket) and keeps the fastest.
+static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int *variant) {
+  if (ctx->forced_variant >= 0) { *variant = ctx->forced_variant; return VQEMPS_OK; }
+  const int key = batch_bucket(B);
+  auto it = h.tuned.find(key);
+  if (it != h.tuned.end()) { *variant = it->second; return VQEMPS_OK; }
+  cudaEvent_t e0, e1;
+  CUDA_TRY(ctx, cudaEventCreate(&e0));
+  CUDA_TRY(ctx, cudaEventCreate(&e1));
+  int best = LV_SIMT4;
+  float best_ms = 1e30f;
+  for (int v = 0; v < LV_COUNT; ++v) {
+    int rc = run_levels(ctx, h, B, st, v);      // warm
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaEventRecord(e0, st));
+    rc = run_levels(ctx, h, B, st, v);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaEventRecord(e1, st));
+    CUDA_TRY(ctx, cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CUDA_TRY(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) { best_ms = ms; best = v; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h.tuned[key] = best;
+  *variant = best;
+  return VQEMPS_OK;
+}
+
+// Trie levels and the energy reduction on the prepared states (needs launch_right first).
+static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
+                         double *energies_dev, double *per_term_dev) {
+  const int nleaf = std::max(h.nleaf, 1);
+  CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
+  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * h.max_slot * ENV_ELEMS));
+  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * h.max_slot * ENV_ELEMS));
+  int variant = LV_SIMT4;
+  int rc = pick_variant(ctx, h, B, st, &variant);
+  if (rc) return rc;
+  rc = run_levels(ctx, h, B, st, variant);
+  if (rc) return rc;
   reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h.d_leaf_coef, h.nleaf,
                                              h.d_term_leaf, h.T, ctx->status.ptr, energies_dev,
                                              per_term_dev);
@@ -676,9 +764,27 @@ static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st
   return VQEMPS_OK;
 }
 
+// Force a level kernel variant (0 SIMT, 1 DMMA x4 warps, 2 DMMA x8 warps) or
+// restore autotuning (-1); query the variant a plan uses for a batch size.
+extern "C" int vqemps_set_level_variant(vqemps_ctx *ctx, int variant) {
+  if (!ctx || variant < -1 || variant >= LV_COUNT) return VQEMPS_INVALID;
+  ctx->forced_variant = variant;
+  return VQEMPS_OK;
+}
+
 static Hamiltonian *find_ham(vqemps_ctx *ctx, int handle) {
   auto it = ctx->hams.find(handle);
   return it == ctx->hams.end() ? nullptr : it->second.get();
+}
+
+extern "C" int vqemps_level_variant(vqemps_ctx *ctx, int handle, int B, int *variant) {
+  if (!ctx || !variant) return VQEMPS_INVALID;
+  Hamiltonian *h = find_ham(ctx, handle);
+  if (!h) return VQEMPS_INVALID;
+  if (ctx->forced_variant >= 0) { *variant = ctx->forced_variant; return VQEMPS_OK; }
+  auto it = h->tuned.find(batch_bucket(B));
+  *variant = it == h->tuned.end() ? -1 : it->second;
+  return VQEMPS_OK;
 }
 
 extern "C" int vqemps_energy_batch(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,

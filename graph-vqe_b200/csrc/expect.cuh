@@ -250,6 +250,167 @@ level_kernel(LevelParams p) {
 }
 
 // ---------------------------------------------------------------------------
+// Prefetching variant: persistent warps walk several parents each. A warp owns a
+// 4 KiB parent slot and an 8 KiB S panel; as soon as the first half of a parent
+// is done the next parent's environment is copied into the slot with cp.async
+// (16 bytes per lane per instruction), overlapping the second half. The CTA
+// stages R_{s+1} next to the site tile. Same arithmetic and lane layout as
+// level_kernel.
+// ---------------------------------------------------------------------------
+constexpr int PF_WARPS = 4;
+
+struct LevelPfSmem {
+  cplx A[SITE_ELEMS];
+  cplx R[ENV_ELEMS];
+  cplx E[PF_WARPS][ENV_ELEMS];          // per warp: parent environment slot
+  cplx S[PF_WARPS][2 * ENV_ELEMS];      // per warp: S_0 | S_1
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Stage the parent environment of group g into E (cp.async, or the root identity).
+__device__ __forceinline__ void stage_parent(const LevelParams &p, int b, int g, cplx *E, int lane) {
+  const DevGroup grp = p.groups[g];
+  if (grp.parent_slot < 0) {
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
+  } else {
+    const cplx *src = p.env_prev + ((size_t)b * p.nslot_prev + grp.parent_slot) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) cp_async16(E + e, src + e);
+  }
+}
+
+__global__ void __launch_bounds__(PF_WARPS * 32, 3)
+level_pf_kernel(LevelParams p, int groups_per_warp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LevelPfSmem &sm = *reinterpret_cast<LevelPfSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += PF_WARPS * 32) sm.A[e] = ag[e];
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += PF_WARPS * 32) sm.R[e] = rg[e];
+  }
+  __syncthreads();
+  const cplx *A = sm.A;
+  const cplx *R = sm.R;
+  const int rq = lane >> 3, cq = lane & 7;
+  // this warp's parents: first, first + stride, ... (at most groups_per_warp)
+  const int stride = gridDim.x * PF_WARPS;
+  const int first = blockIdx.x * PF_WARPS + warp;
+  int count = 0;
+  if (first < p.ngroups) count = min(groups_per_warp, (p.ngroups - first + stride - 1) / stride);
+  if (count == 0) return;
+  cplx *E = sm.E[warp];
+  cplx *S = sm.S[warp];
+  stage_parent(p, b, first, E, lane);
+  cp_async_commit();
+  for (int k = 0; k < count; ++k) {
+    const int gidx = first + k * stride;
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    {
+      cplx acc[4][4];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[r][c] = cmake(0, 0);
+#pragma unroll 1
+      for (int kk = 0; kk < CHI; ++kk) {
+        cplx e[4], a[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) e[r] = E[(rq * 4 + r) * CHI + kk];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) a[c] = A[kk * 2 * CHI + cq + 8 * c];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) cfma(acc[r][c], e[r], a[c]);
+      }
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          S[(c >> 1) * ENV_ELEMS + (rq * 4 + r) * CHI + cq + 8 * (c & 1)] = acc[r][c];
+    }
+    __syncwarp();   // E is dead and S is complete: prefetch the next parent
+    if (k + 1 < count) stage_parent(p, b, gidx + stride, E, lane);
+    cp_async_commit();
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      cplx t0[4][2], t1[4][2];
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) { t0[r][c] = cmake(0, 0); t1[r][c] = cmake(0, 0); }
+      const int s0 = cls == 0 ? 0 : 1;
+      const int s1 = cls == 0 ? 1 : 0;
+#pragma unroll 1
+      for (int a = 0; a < CHI; ++a) {
+        cplx sv0[2], sv1[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          sv0[c] = S[s0 * ENV_ELEMS + a * CHI + cq + 8 * c];
+          sv1[c] = S[s1 * ENV_ELEMS + a * CHI + cq + 8 * c];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const cplx av0 = A[(a * 2 + 0) * CHI + rq * 4 + r];
+          const cplx av1 = A[(a * 2 + 1) * CHI + rq * 4 + r];
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            cfma_conj(t0[r][c], av0, sv0[c]);
+            cfma_conj(t1[r][c], av1, sv1[c]);
+          }
+        }
+      }
+      for (int ci = 0; ci < grp.nchild; ++ci) {
+        const DevNode node = p.nodes[grp.child_begin + ci];
+        const bool iz = (node.code == 0 || node.code == 3);
+        if (iz != (cls == 0)) continue;
+        cplx out[4][2];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            if (node.code == 0 || node.code == 1) out[r][c] = cadd(t0[r][c], t1[r][c]);
+            else if (node.code == 3) out[r][c] = csub(t0[r][c], t1[r][c]);
+            else { const cplx d = csub(t1[r][c], t0[r][c]); out[r][c] = cmake(-d.y, d.x); }
+          }
+        if (node.env_slot >= 0) {
+          cplx *dst = p.env_cur + ((size_t)b * p.nslot_cur + node.env_slot) * ENV_ELEMS;
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) dst[(rq * 4 + r) * CHI + cq + 8 * c] = out[r][c];
+        }
+        if (node.leaf >= 0) {
+          double v = 0.0;
+#pragma unroll
+          for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const cplx rv = R[(rq * 4 + r) * CHI + cq + 8 * c];
+              v += out[r][c].x * rv.x - out[r][c].y * rv.y;
+            }
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) p.leafval[(size_t)b * p.nleaf_total + node.leaf] = v;
+        }
+      }
+    }
+    __syncwarp();   // S is rewritten by the next parent
+  }
+  cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
 // energies[b] = sum_leaf coef[leaf] * value[b, leaf] (fixed-order tree sum),
 // per_term[b, t] = value[b, term_leaf[t]]. Failed states give NaN.
 // ---------------------------------------------------------------------------

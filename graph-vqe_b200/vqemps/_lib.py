@@ -27,7 +27,7 @@ SYMBOLS = (
     "vqemps_free_hamiltonian", "vqemps_energy_batch", "vqemps_energy_batch_host",
     "vqemps_batch_status", "vqemps_energy_grad_batch", "vqemps_sample",
     "vqemps_sampled_energy", "vqemps_copy_sites", "vqemps_plan_stats", "vqemps_profile_energy",
-    "vqemps_energy_noalloc",
+    "vqemps_energy_noalloc", "vqemps_set_level_variant", "vqemps_level_variant",
 )
 
 
@@ -78,6 +78,8 @@ def load():
         "vqemps_plan_stats": (I, [P, I, ctypes.POINTER(D)]),
         "vqemps_profile_energy": (I, [P, I, V, I, ctypes.POINTER(D), ctypes.POINTER(I), V]),
         "vqemps_energy_noalloc": (I, [P, I, V, V, V, V, V]),
+        "vqemps_set_level_variant": (I, [P, I]),
+        "vqemps_level_variant": (I, [P, I, I, ctypes.POINTER(I)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -165,6 +165,18 @@ class Engine:
             len(words), ctypes.byref(h)), "set_hamiltonian")
         return Hamiltonian(h.value, self.n, len(words), words, coeffs)
 
+    LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf")
+
+    def set_level_variant(self, variant):
+        """Force a trie-level kernel ('simt', 'dmma4', 'dmma8', 'simt_pf', 'dmma_pf') or None to autotune."""
+        v = -1 if variant is None else self.LEVEL_VARIANTS.index(variant)
+        check(self.ctx, self.lib.vqemps_set_level_variant(self.ctx, v), "set_level_variant")
+
+    def level_variant(self, ham: Hamiltonian, B: int):
+        v = ctypes.c_int()
+        check(self.ctx, self.lib.vqemps_level_variant(self.ctx, ham.handle, B, ctypes.byref(v)), "level_variant")
+        return None if v.value < 0 else self.LEVEL_VARIANTS[v.value]
+
     def plan_stats(self, ham: Hamiltonian) -> dict:
         out = (ctypes.c_double * 6)()
         check(self.ctx, self.lib.vqemps_plan_stats(self.ctx, ham.handle, out), "plan_stats")

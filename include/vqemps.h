@@ -160,6 +160,18 @@ int vqemps_sampled_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, 
                           uint64_t seed, int rng, int mode, double *energies_dev,
                           double *per_term_dev, void *stream);
 
+/* Level-kernel selection (no reference counterpart). The trie levels have five
+ * implementations: 0 FP64 CUDA-core (SIMT) kernel, 1 FP64 tensor-core (DMMA)
+ * kernel with 4 warps per CTA, 2 DMMA with 8 warps per CTA, 3 SIMT with
+ * persistent warps that prefetch the next parent environment (cp.async),
+ * 4 DMMA with the same prefetching pipeline. By default the
+ * engine times each once per plan and batch-size bucket (powers of two) on the
+ * first call and keeps the fastest (that first call synchronises its stream);
+ * vqemps_set_level_variant forces one (-1 restores tuning);
+ * vqemps_level_variant reports the one in use (-1: not tuned yet). */
+int vqemps_set_level_variant(vqemps_ctx *ctx, int variant);
+int vqemps_level_variant(vqemps_ctx *ctx, int handle, int B, int *variant);
+
 /* Benchmark support (no reference counterpart): phase times of one batched
  * energy call -- ms[0] state preparation, ms[1] right environments, ms[2] trie
  * levels, ms[3] energy reduction -- and the number of kernels one call launches.
