@@ -13,12 +13,16 @@
 // per-site 2x2 matrix in shared memory and are folded into the next two-site
 // gate's 4x4 matrix (or applied at the end). Each two-site gate builds
 // Theta = G (A (x) B) (2Dl x 2Dr, <= 32 x 32 complex) in shared memory and
-// factors it with an FP64 one-sided Jacobi SVD that orthogonalises the ROWS of
-// Theta by left unitary rotations: V^H Theta = X with orthogonal rows, so the
-// new left site V[:, kept] is unitary to rounding (no division by small
-// singular values, null directions included) and the right site is the kept
-// rows of X = S * Vh. Rows are kept by descending norm, exactly the gesvd
-// ordering the reference uses.
+// factors it with an FP64 one-sided Jacobi SVD on its shorter side. For a wide
+// or square Theta the ROWS are orthogonalised by left unitary rotations,
+// V^H Theta = X, so the new left site V[:, kept] is unitary to rounding (no
+// division by small singular values, null directions included) and the right
+// site is the kept rows of X = S * Vh. For a tall Theta (the left-to-right
+// sweeps at full bond: 32 x 16) the same rotations act on Theta^T, halving the
+// vectors and quartering the rotation steps; the left site is then the
+// normalised rotated columns, re-orthogonalised against each other where a
+// singular value is numerically zero. Singular values are kept in descending
+// order, the gesvd ordering the reference uses.
 #pragma once
 #include "common.cuh"
 
@@ -146,6 +150,10 @@ evolve_kernel(EvolveParams p) {
     const int s = g.site;
     const int dl = BOND[s], dc = BOND[s + 1], dr = BOND[s + 2];
     const int m = 2 * dl, ncol = 2 * dr;
+    // Jacobi runs on the shorter side: the rows of Theta when m <= ncol, the
+    // rows of Theta^T (the columns of Theta) when Theta is tall.
+    const bool tall = m > ncol;
+    const int mr = tall ? ncol : m, mc = tall ? m : ncol;
     {
       const cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       const cplx *gb = ga + SITE_ELEMS;
@@ -184,7 +192,8 @@ evolve_kernel(EvolveParams p) {
         v = cadd(v, cmul(G[IJ * 4 + 2], t10));
         v = cadd(v, cmul(G[IJ * 4 + 3], t11));
         const int I = IJ >> 1, J = IJ & 1;
-        X[(l * 2 + I) * 32 + (J * dr + r)] = v;
+        if (tall) X[(J * dr + r) * 32 + (l * 2 + I)] = v;
+        else X[(l * 2 + I) * 32 + (J * dr + r)] = v;
         fro += cabs2(v);
       }
     }
@@ -213,21 +222,21 @@ evolve_kernel(EvolveParams p) {
     // phase of gamma moved onto row q (V absorbs it). Row norms then move by
     // -+ w |gamma|^2 and are kept in NORM, recomputed exactly after each sweep.
     const int pair = tid >> 4, lane = tid & 15;
-    const int npairs = m >> 1;
-    if (tid < m) {
+    const int npairs = mr >> 1;
+    if (tid < mr) {
       double a = 0.0;
-      for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
+      for (int j = 0; j < mc; ++j) a += cabs2(X[tid * 32 + j]);
       NORM[tid] = a;
     }
     __syncthreads();
     bool converged = false;
     for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
       int rotated = 0;
-      for (int step = 0; step < m - 1; ++step) {
+      for (int step = 0; step < mr - 1; ++step) {
         int pr = 0, qr = 0;
         const bool active = pair < npairs;
         if (active) {
-          const int mm1 = m - 1;
+          const int mm1 = mr - 1;
           if (pair == 0) { pr = 0; qr = 1 + (step % mm1); }
           else { pr = 1 + ((step + pair) % mm1); qr = 1 + ((step + mm1 - pair) % mm1); }
           if (pr > qr) { int t = pr; pr = qr; qr = t; }
@@ -235,8 +244,8 @@ evolve_kernel(EvolveParams p) {
         cplx xp0 = cmake(0, 0), xq0 = cmake(0, 0), xp1 = cmake(0, 0), xq1 = cmake(0, 0);
         const int j0 = lane, j1 = lane + 16;
         if (active) {
-          if (j0 < ncol) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
-          if (j1 < ncol) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
+          if (j0 < mc) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
+          if (j1 < mc) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
         }
         // gamma = sum_j X[p,j] conj(X[q,j])
         double gr = xp0.x * xq0.x + xp0.y * xq0.y + xp1.x * xq1.x + xp1.y * xq1.y;
@@ -254,16 +263,16 @@ evolve_kernel(EvolveParams p) {
           const double c = rsqrt(1.0 + w * w * g2);
           const cplx wg = cmake(w * gr, w * gim);             // w gamma
           const cplx wgc = cconj(wg);                         // w conj(gamma)
-          if (j0 < ncol) {
+          if (j0 < mc) {
             X[pr * 32 + j0] = cscale(csub(xp0, cmul(wg, xq0)), c);
             X[qr * 32 + j0] = cscale(cadd(cmul(wgc, xp0), xq0), c);
           }
-          if (j1 < ncol) {
+          if (j1 < mc) {
             X[pr * 32 + j1] = cscale(csub(xp1, cmul(wg, xq1)), c);
             X[qr * 32 + j1] = cscale(cadd(cmul(wgc, xp1), xq1), c);
           }
           // V <- V J^H: V_p' = c (V_p - w conj(gamma) V_q), V_q' = c (w gamma V_p + V_q)
-          for (int i = lane; i < m; i += 16) {
+          for (int i = lane; i < mr; i += 16) {
             const cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
             VT[pr * 32 + i] = cscale(csub(vp, cmul(wgc, vq)), c);
             VT[qr * 32 + i] = cscale(cadd(cmul(wg, vp), vq), c);
@@ -276,20 +285,20 @@ evolve_kernel(EvolveParams p) {
         __syncthreads();
       }
       converged = !__syncthreads_or(rotated);
-      if (tid < m) {
+      if (tid < mr) {
         double a = 0.0;
-        for (int j = 0; j < ncol; ++j) a += cabs2(X[tid * 32 + j]);
+        for (int j = 0; j < mc; ++j) a += cabs2(X[tid * 32 + j]);
         NORM[tid] = a;
       }
       __syncthreads();
     }
     // ---- singular values = row norms, sorted descending (stable in row index) ----
-    if (tid < m) NORM[tid] = sqrt(NORM[tid]);
+    if (tid < mr) NORM[tid] = sqrt(NORM[tid]);
     __syncthreads();
-    if (tid < m) {
+    if (tid < mr) {
       const double v = NORM[tid];
       int rank = 0;
-      for (int q = 0; q < m; ++q) {
+      for (int q = 0; q < mr; ++q) {
         const double w = NORM[q];
         rank += (w > v) || (w == v && q < tid);
       }
@@ -299,12 +308,12 @@ evolve_kernel(EvolveParams p) {
     __syncthreads();
     // ---- selectDirectSvdRank (dist_svd.cuh:194-212) ----
     if (tid == 0) {
-      const int r = m < ncol ? m : ncol;
+      const int r = mr;                          // min(m, ncol)
       int st = converged ? ST_OK : ST_NONFINITE;
       int selected = 0;
       const double thr = fmax(p.abs_cut, p.rel_cut * SIG[0]);
       const bool zero_cut = (p.abs_cut == 0.0 && p.rel_cut == 0.0);
-      for (int i = 0; i < m; ++i)
+      for (int i = 0; i < mr; ++i)
         if (!isfinite(NORM[i])) st = ST_NONFINITE;
       for (int i = 0; i < r; ++i)
         if (zero_cut || SIG[i] > thr) ++selected;
@@ -319,8 +328,9 @@ evolve_kernel(EvolveParams p) {
     __syncthreads();
     if (MISC[0] != ST_OK) break;
     const int k = MISC[1];
-    // ---- pack: left = V[:, perm[:k]] (Dl,2,k); right = X[perm[:k], :] (k,2,Dr) ----
-    {
+    // ---- pack (left = U_k (Dl,2,k), right = S_k Vh_k (k,2,Dr), packDirectSvdFactors) ----
+    if (!tall) {
+      // Theta = V X: left = V[:, perm[:k]], right = X[perm[:k], :]
       cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       cplx *gb = ga + SITE_ELEMS;
       for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) {
@@ -328,6 +338,55 @@ evolve_kernel(EvolveParams p) {
         ga[e] = (l < dl && c < k) ? VT[PERM[c] * 32 + (l * 2 + I)] : cmake(0, 0);
         const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
         gb[e] = (cc < k && r < dr) ? X[PERM[cc] * 32 + (J * dr + r)] : cmake(0, 0);
+      }
+    } else {
+      // Theta^T = V X, so Theta = X^T V^T: left column c = X[perm[c], :] / sigma_c,
+      // right row c = sigma_c V[:, perm[c]]^T. Columns whose sigma is numerically
+      // zero (<= 64 eps r sigma_0, the rank guard's scale) carry no weight; they are
+      // replaced by unit vectors made orthogonal to the kept columns (two
+      // Gram-Schmidt passes) so that the left site stays an isometry, as gesvd's
+      // orthonormal completion does in the reference.
+      cplx *UC = SA;                                   // k x m, UC[c * 32 + row]
+      const double tiny = 64.0 * eps * mr * SIG[0];
+      for (int e = tid; e < k * 32; e += EVOLVE_THREADS) {
+        const int c = e >> 5, row = e & 31;
+        UC[e] = (row < m && SIG[c] > tiny) ? cscale(X[PERM[c] * 32 + row], 1.0 / SIG[c]) : cmake(0, 0);
+      }
+      __syncthreads();
+      if (!(SIG[k - 1] > tiny) && tid < 32) {
+        for (int c = 0; c < k; ++c) {
+          if (SIG[c] > tiny) continue;
+          for (int row0 = 0; row0 < m; ++row0) {
+            cplx v = cmake(tid == row0 ? 1.0 : 0.0, 0.0);
+            for (int pass = 0; pass < 2; ++pass)
+              for (int i = 0; i < c; ++i) {
+                const cplx u = tid < m ? UC[i * 32 + tid] : cmake(0, 0);
+                double dr_ = u.x * v.x + u.y * v.y, di = u.x * v.y - u.y * v.x;   // conj(u) v
+                for (int o = 16; o > 0; o >>= 1) {
+                  dr_ += __shfl_xor_sync(0xffffffffu, dr_, o);
+                  di += __shfl_xor_sync(0xffffffffu, di, o);
+                }
+                v = csub(v, cmul(cmake(dr_, di), u));
+              }
+            double nn = cabs2(v);
+            for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+            // some basis vector keeps at least the average residual (m - c) / m
+            if (nn > 0.5 * (double)(m - c) / m) {
+              if (tid < m) UC[c * 32 + tid] = cscale(v, 1.0 / sqrt(nn));
+              __syncwarp();
+              break;
+            }
+          }
+        }
+      }
+      __syncthreads();
+      cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
+      cplx *gb = ga + SITE_ELEMS;
+      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) {
+        const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
+        ga[e] = (l < dl && c < k) ? UC[c * 32 + (l * 2 + I)] : cmake(0, 0);
+        const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
+        gb[e] = (cc < k && r < dr) ? cscale(VT[PERM[cc] * 32 + (J * dr + r)], SIG[cc]) : cmake(0, 0);
       }
     }
     if (tid == 0) BOND[s + 1] = k;

@@ -198,3 +198,22 @@ def test_config_40q_batch_energy_parity_sample(vq, variant):
         ref = float(np.dot(O.expect_words(O.svd_evolve(spec, thetas[b], 16), words).real, coeffs))
         assert abs(e[b] - ref) <= RTOL * max(1.0, abs(ref))
     assert np.all(np.isfinite(e))
+
+
+@pytest.mark.parametrize("pattern", ["linear", "reverse_linear"])
+@pytest.mark.parametrize("order", ["msb", "qubit"])
+def test_degenerate_angles_keep_isometric_sites(vq, pattern, order):
+    """Zero and pi angles make Theta rank deficient (product or classical states):
+    the left sites must stay isometries and the state must stay exact."""
+    spec = O.hardware_efficient_spec(10, 4, ("ry",), pattern)
+    rng = np.random.default_rng(9)
+    for x in (np.zeros(spec["count"]), np.pi * rng.integers(0, 2, spec["count"]).astype(float),
+              np.where(rng.random(spec["count"]) < 0.5, 0.0, rng.uniform(-np.pi, np.pi, spec["count"]))):
+        eng = _engine(vq, spec, 16, order)
+        ham = eng.set_hamiltonian(["Z" + "I" * 9, "IXXIIIIIII", "IIIIIYZIIX"], [1.0, 0.5, -0.25])
+        eng.energy(ham, x)
+        dims = eng.bond_dims()
+        raw = eng.sites(0)
+        sites = [raw[s, :dims[s], :, :dims[s + 1]] for s in range(10)]
+        psi = O.statevector(O.reverse_chain(sites) if order == "msb" else sites)
+        np.testing.assert_allclose(psi, O.dense_statevector(spec, x), atol=1e-11)
