@@ -84,7 +84,7 @@ def barrier(dist, device):
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -94,13 +94,19 @@ class ClockSampler:
         self.path = Path(os.environ.get("VQEMPS_CLOCKS_FILE", f"/tmp/vqemps_clocks_{os.getpid()}.csv"))
 
     def start(self):
+        """Start sampling every 50 ms; give nvidia-smi time to produce its first rows."""
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.5)
         except (OSError, FileNotFoundError):
             self.proc = None
+
+    def window(self, t0, t1):
+        """Timed region as wall-clock datetimes (samples outside it are dropped)."""
+        self.t0, self.t1 = t0, t1
 
     def stop(self):
         if self.proc is None:
@@ -108,19 +114,28 @@ class ClockSampler:
         self.proc.terminate()
         self.proc.wait(timeout=10)
         self.fh.close()
-        rows = [r.split(",") for r in self.path.read_text().strip().splitlines() if r.strip()]
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        import datetime
+        rows = [[c.strip() for c in r.split(",")] for r in self.path.read_text().strip().splitlines() if r.strip()]
+        kept = []
+        for r in rows:
+            if len(r) < 10:
+                continue
+            try:
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f")
+            except ValueError:
+                continue
+            if getattr(self, "t0", None) is None or self.t0 <= ts <= self.t1:
+                kept.append(r)
+        sm = [float(r[2]) for r in kept if r[2].replace(".", "").isdigit()]
+        smax = [float(r[3]) for r in kept if r[3].replace(".", "").isdigit()]
         reasons = set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for r in rows:
-            if len(r) < 9:
-                continue
-            for name, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
+        for r in kept:
+            for name, v in zip(names, r[6:10]):
+                if v.lower() == "active":
                     reasons.add(name)
         return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=max(smax) if smax else None,
-                    reasons=sorted(reasons), samples=len(rows))
+                    reasons=sorted(reasons), samples=len(kept))
 
 
 def measure_fp64_peak(torch, device):
@@ -142,6 +157,19 @@ def measure_fp64_peak(torch, device):
     del a, b
     torch.cuda.empty_cache()
     return best
+
+
+def profiled_traffic(variant):
+    """DRAM bytes per evaluation of all trie levels, from the committed ncu summary
+    of the same kernel (profiles/level_mma_pf_kernel_40q.md: sum of
+    dram__bytes_read.sum + dram__bytes_write.sum over the 40 level launches of one
+    step at B = 32, divided by 32); None for kernels without such a capture."""
+    path = ROOT / "profiles" / "level_mma_pf_kernel_40q.md"
+    if variant != "dmma_pf" or not path.exists():
+        return None
+    import re
+    m = re.search(r"traffic_bytes_per_eval:\s*([0-9.eE+]+)", path.read_text())
+    return float(m.group(1)) if m else None
 
 
 def cpu_reference_rate(seconds, threads):
@@ -218,12 +246,15 @@ def main():
     barrier(dist, device)
     torch.cuda.synchronize()
     clocks.start()
+    import datetime
+    wall0 = datetime.datetime.now()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     for _ in range(args.steps):
         step()
     end.record(stream)
     end.synchronize()
+    clocks.window(wall0, datetime.datetime.now())
     clock_info = clocks.stop()
     barrier(dist, device)
     elapsed = start.elapsed_time(end) * 1e-3
@@ -242,8 +273,10 @@ def main():
     variant = eng.level_variant(ham, args.batch)
     kernel = {"simt": "level_kernel (FP64 FMA pipes)", "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
               "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)"}.get(variant, str(variant))
+    traffic = profiled_traffic(variant)
     roofline = dict(bound="tensor" if variant and variant.startswith("dmma") else "fp64", achieved=achieved,
-                    peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak, traffic=None,
+                    peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
+                    traffic=traffic * args.batch if traffic else None,
                     kernel=kernel + ", all trie levels of one step",
                     peak_source="cuBLAS FP64 DGEMM 8192^3 (DMMA tensor cores) measured in this run, burst",
                     survey_unit_tflops=stats["flops_survey"] * args.batch / level_s / 1e12)

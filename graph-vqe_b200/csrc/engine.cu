@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -173,6 +174,13 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(level_mma_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelMmaPfSmem));
   grad_set_attributes();
+  // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the
+  // autotuner's timings are meaningless under a serialising profiler.
+  if (const char *v = std::getenv("VQEMPS_LEVEL_VARIANT")) {
+    static const char *names[] = {"simt", "dmma4", "dmma8", "simt_pf", "dmma_pf"};
+    for (int i = 0; i < 5; ++i)
+      if (std::strcmp(v, names[i]) == 0 || (v[0] == '0' + i && v[1] == 0)) ctx->forced_variant = i;
+  }
   *out = ctx;
   return VQEMPS_OK;
 }

@@ -168,7 +168,9 @@ int vqemps_sampled_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, 
  * engine times each once per plan and batch-size bucket (powers of two) on the
  * first call and keeps the fastest (that first call synchronises its stream);
  * vqemps_set_level_variant forces one (-1 restores tuning);
- * vqemps_level_variant reports the one in use (-1: not tuned yet). */
+ * vqemps_level_variant reports the one in use (-1: not tuned yet). The
+ * environment variable VQEMPS_LEVEL_VARIANT (simt, dmma4, dmma8, simt_pf,
+ * dmma_pf or 0-4), read by vqemps_create, forces one for every context. */
 int vqemps_set_level_variant(vqemps_ctx *ctx, int variant);
 int vqemps_level_variant(vqemps_ctx *ctx, int handle, int B, int *variant);
 
