@@ -118,10 +118,11 @@ struct vqemps_ctx {
   DevBuf<int32_t> zsum;
   DevBuf<cplx> branch;
   DevBuf<double> analytic_stage;
-  DevBuf<cplx> grad_sites, grad_envs, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
+  DevBuf<cplx> grad_sites, grad_envs, grad_seg, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
   DevBuf<double> grad_stage;
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
+  int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
@@ -196,7 +197,7 @@ extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
   ctx->analytic_stage.release();
   ctx->grad_sites.release(); ctx->grad_envs.release(); ctx->grad_bar0.release();
   ctx->grad_bar1.release(); ctx->grad_sitebar.release(); ctx->grad_stage.release();
-  ctx->grad_partial.release(); ctx->grad_leafsum.release();
+  ctx->grad_partial.release(); ctx->grad_leafsum.release(); ctx->grad_seg.release();
   delete ctx;
   return VQEMPS_OK;
 }

@@ -10,9 +10,12 @@
 //   therefore evolves independently of its neighbours, so a CTA per
 //   (state, site) replays that site's own event list (one-site gates and its
 //   half of each CX).
-// * Energy. The same shared-prefix trie as the analytic path; every level's
-//   environments are kept (they are the checkpoints of the backward sweep) and
-//   each CTA sums c_leaf * E_leaf of its leaves per level.
+// * Energy. The same shared-prefix trie as the analytic path. The forward sweep
+//   keeps the environments of every K-th level only (checkpoints; K = 1 keeps
+//   all) and each CTA sums c_leaf * E_leaf of its leaves per level. The
+//   backward sweep walks segments of K levels from the last: it recomputes the
+//   segment's K - 1 inner levels from the checkpoint before it, then runs the
+//   segment's backward levels.
 // * Backward through the trie. For a parent E with children x and cotangents
 //   Ebar_x (Re<Ebar, dE> convention): D_00 = Ebar_I + Ebar_Z, D_11 = Ebar_I - Ebar_Z,
 //   D_01 = Ebar_X + i Ebar_Y, D_10 = Ebar_X - i Ebar_Y;
@@ -156,9 +159,11 @@ constexpr int GROUPS_PER_WARP = 4;
 struct GradLevelParams {
   const cplx *sites;
   const cplx *right;
-  cplx *env_all;            // B x total_slots x ENV_ELEMS
-  size_t total_slots;
-  int slot_prev, slot_cur;  // level offsets into the slot space (-1 prev at s = 0)
+  const cplx *env_prev;     // environments of level s-1 for state 0 (unused at s = 0)
+  size_t prev_stride;       // elements between consecutive states
+  cplx *env_cur;            // where level s environments go (state 0)
+  size_t cur_stride;
+  int leaf_work;            // forward: 1 computes leaf values and leaf sums, 0 only environments
   const DevGroup *groups;
   const DevNode *nodes;
   const double *leaf_coef;
@@ -231,7 +236,7 @@ grad_fwd_level_kernel(GradLevelParams p) {
     if (grp.parent_slot < 0) {
       for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
     } else {
-      const cplx *src = p.env_all + ((size_t)b * p.total_slots + p.slot_prev + grp.parent_slot) * ENV_ELEMS;
+      const cplx *src = p.env_prev + (size_t)b * p.prev_stride + (size_t)grp.parent_slot * ENV_ELEMS;
       for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = src[e];
     }
     __syncwarp();
@@ -272,13 +277,13 @@ grad_fwd_level_kernel(GradLevelParams p) {
             else { const cplx d = csub(t1[r][c], t0[r][c]); out[r][c] = cmake(-d.y, d.x); }
           }
         if (node.env_slot >= 0) {
-          cplx *dst = p.env_all + ((size_t)b * p.total_slots + p.slot_cur + node.env_slot) * ENV_ELEMS;
+          cplx *dst = p.env_cur + (size_t)b * p.cur_stride + (size_t)node.env_slot * ENV_ELEMS;
 #pragma unroll
           for (int r = 0; r < 4; ++r)
 #pragma unroll
             for (int c = 0; c < 2; ++c) dst[(rb * 4 + r) * CHI + cb * 2 + c] = out[r][c];
         }
-        if (node.leaf >= 0) {
+        if (node.leaf >= 0 && p.leaf_work) {
           const double cf = p.leaf_coef[node.leaf];
           double v = 0.0;
 #pragma unroll
@@ -298,6 +303,7 @@ grad_fwd_level_kernel(GradLevelParams p) {
     __syncwarp();
   }
   __syncthreads();
+  if (!p.leaf_work) return;
   // fixed-order combination of the warps' leaf sums
   cplx *dst = p.partial + ((size_t)b * gridDim.x + blockIdx.x) * ENV_ELEMS;
   for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) {
@@ -407,7 +413,7 @@ grad_bwd_level_kernel(GradLevelParams p) {
     if (grp.parent_slot < 0) {
       for (int e = lane; e < ENV_ELEMS; e += 32) C[e] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
     } else {
-      const cplx *src = p.env_all + ((size_t)b * p.total_slots + p.slot_prev + grp.parent_slot) * ENV_ELEMS;
+      const cplx *src = p.env_prev + (size_t)b * p.prev_stride + (size_t)grp.parent_slot * ENV_ELEMS;
       for (int e = lane; e < ENV_ELEMS; e += 32) C[e] = src[e];
     }
     __syncwarp();

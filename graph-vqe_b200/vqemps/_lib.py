@@ -28,6 +28,7 @@ SYMBOLS = (
     "vqemps_batch_status", "vqemps_energy_grad_batch", "vqemps_sample",
     "vqemps_sampled_energy", "vqemps_copy_sites", "vqemps_plan_stats", "vqemps_profile_energy",
     "vqemps_energy_noalloc", "vqemps_set_level_variant", "vqemps_level_variant",
+    "vqemps_set_grad_checkpoint",
 )
 
 
@@ -79,6 +80,7 @@ def load():
         "vqemps_profile_energy": (I, [P, I, V, I, ctypes.POINTER(D), ctypes.POINTER(I), V]),
         "vqemps_energy_noalloc": (I, [P, I, V, V, V, V, V]),
         "vqemps_set_level_variant": (I, [P, I]),
+        "vqemps_set_grad_checkpoint": (I, [P, I]),
         "vqemps_level_variant": (I, [P, I, I, ctypes.POINTER(I)]),
     }
     for name, (res, args) in sig.items():

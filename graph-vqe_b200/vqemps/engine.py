@@ -221,6 +221,10 @@ class Engine:
               "energy_batch_host")
         return out_host
 
+    def set_grad_checkpoint(self, every: int):
+        """Keep every `every`-th trie level in the gradient's forward sweep (1: all)."""
+        check(self.ctx, self.lib.vqemps_set_grad_checkpoint(self.ctx, int(every)), "set_grad_checkpoint")
+
     def energy_grad(self, ham: Hamiltonian, theta, stream=None):
         """Energies and dE/dtheta through the exact bond-doubling MPS."""
         t = self._theta(theta)

@@ -133,6 +133,12 @@ int vqemps_batch_status(vqemps_ctx *ctx, int32_t *status, int B, void *stream);
 int vqemps_energy_grad_batch(vqemps_ctx *ctx, int handle, const double *theta_dev, int B,
                              double *energies_dev, double *grad_dev, void *stream);
 
+/* Environment checkpointing of the gradient (no reference counterpart; the
+ * reference bounds memory by 128-term chunks, reverse_mps.py:91-96): the forward
+ * sweep keeps every `every`-th level, the backward sweep recomputes the rest one
+ * segment at a time. Default 8; 1 keeps every level (no recomputation). */
+int vqemps_set_grad_checkpoint(vqemps_ctx *ctx, int every);
+
 /* Perfect sampling of B states: shots bitstrings each, bit q of shot s of state
  * b in packed_dev[(b * shots + s) * W + q / 64] >> (q % 64), W = ceil(n / 64),
  * QUBIT order, n <= 256. Replaces sample() without noise

@@ -28,9 +28,11 @@ def _spec(case):
 
 @pytest.mark.parametrize("case", [c for c in GOLDEN if c["gradient"] is not None], ids=lambda c: c["name"])
 @pytest.mark.parametrize("order", ["msb", "qubit"])
-def test_gradient_matches_reference_golden(vq, case, order):
+@pytest.mark.parametrize("every", [1, 3, 8])
+def test_gradient_matches_reference_golden(vq, case, order, every):
     spec = _spec(case)
     eng = vq.Engine(0, 16)
+    eng.set_grad_checkpoint(every)
     eng.set_spec(spec, site_order=order)
     ham = eng.set_hamiltonian(case["words"], case["coeffs"])
     e, g = eng.energy_grad(ham, np.array(case["x"]))
@@ -74,3 +76,18 @@ def test_gradient_with_identity_and_offdiagonal_terms(vq):
     eref, gref = O.reverse_value_gradient(spec, words, coeffs, x)
     assert abs(float(e[0]) - eref) < 1e-12
     np.testing.assert_allclose(g[0].cpu().numpy(), gref, atol=1e-11)
+
+
+def test_checkpointing_is_bitwise_neutral(vq):
+    """Recomputed environments are the same numbers: every interval gives the same bits."""
+    spec, words, coeffs, theta = W.plain_12q(4)
+    out = []
+    for every in (1, 2, 5, 8, 40):
+        eng = vq.Engine(0, 16)
+        eng.set_grad_checkpoint(every)
+        eng.set_spec(spec)
+        ham = eng.set_hamiltonian(words, coeffs)
+        e, g = eng.energy_grad(ham, np.stack([theta, -theta]))
+        out.append((e.cpu().numpy(), g.cpu().numpy()))
+    for e, g in out[1:]:
+        assert np.array_equal(e, out[0][0]) and np.array_equal(g, out[0][1])
