@@ -68,6 +68,44 @@ struct Hamiltonian {
   }
 };
 
+// A partition set: K independent circuits with their own widths, parameters
+// and Hamiltonians, evaluated together in one batch. Per-partition tables sit
+// at fixed strides (widest partition, most terms, most leaves); the trie
+// levels of all partitions are merged level by level, so one launch per level
+// runs every partition's own plan through a work list.
+struct PartSet {
+  int K = 0, n_max = 0, P_max = 0, T_max = 1, leaf_stride = 1, W = 1;
+  int site_order = 0;
+  bool all_diagonal = true;
+  cplx init0, init1;
+  std::vector<int32_t> part_n, part_P, part_T, part_nleaf, part_idleaf, part_gate_off;
+  std::vector<int> lvl_group_off, lvl_node_off, lvl_nslot;   // merged levels (n_max + 1 / n_max)
+  std::vector<int32_t> lvl_pg_begin, lvl_pg_count;           // [s * K + k]: partition k's groups in level s
+  int nlevels = 0;
+  double flops = 0.0;                                        // one evaluation of every partition
+  std::vector<int> bonds;                                    // K x (n_max + 1) allocation bounds
+  DevGate *d_gates = nullptr;
+  cplx *d_mats = nullptr;
+  DevGroup *d_groups = nullptr;
+  DevNode *d_nodes = nullptr;
+  int32_t *d_part = nullptr;        // part_n | part_T | part_nleaf | part_idleaf | part_gate_off (K+1)
+  double *d_leaf_coef = nullptr;    // K x leaf_stride
+  int32_t *d_term_leaf = nullptr;   // K x T_max
+  uint64_t *d_zmask = nullptr;      // K x T_max x W
+  double *d_coeffs = nullptr;       // K x T_max
+  int32_t *d_sumidx = nullptr;      // K x T_max: t for I/Z words, -1 for X/Y words
+  // per-copies cache: state -> partition map and the level work lists
+  int cached_copies = 0;
+  std::vector<int> work_off;        // nlevels + 1 (items)
+  int32_t *d_st_part = nullptr;
+  int32_t *d_work = nullptr;
+  ~PartSet() {
+    cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_part);
+    cudaFree(d_leaf_coef); cudaFree(d_term_leaf); cudaFree(d_zmask); cudaFree(d_coeffs);
+    cudaFree(d_sumidx); cudaFree(d_st_part); cudaFree(d_work);
+  }
+};
+
 template <typename T>
 struct DevBuf {
   T *ptr = nullptr;
@@ -109,6 +147,7 @@ struct vqemps_ctx {
   int32_t *d_ev_off = nullptr, *d_ev_dims = nullptr, *d_slot_off = nullptr, *d_slot_list = nullptr;
   // hamiltonians
   std::map<int, std::unique_ptr<Hamiltonian>> hams;
+  std::map<int, std::unique_ptr<PartSet>> parts;
   int next_handle = 1;
   // workspaces
   DevBuf<cplx> sites, right, env0, env1;
@@ -190,6 +229,7 @@ extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
   if (!ctx) return VQEMPS_OK;
   cudaSetDevice(ctx->device);
   ctx->hams.clear();
+  ctx->parts.clear();
   ctx->sites.release(); ctx->right.release(); ctx->env0.release(); ctx->env1.release();
   ctx->bonds_ws.release(); ctx->status.release(); ctx->leafval.release();
   ctx->theta_stage.release(); ctx->energy_stage.release(); ctx->per_term_stage.release();
@@ -921,4 +961,5 @@ extern "C" int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, voi
 
 #include "engine_sample.inc"
 #include "engine_grad.inc"
+#include "engine_parts.inc"
 #include "noalloc.cu"

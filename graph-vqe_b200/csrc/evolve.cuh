@@ -54,6 +54,13 @@ struct EvolveParams {
   cplx init0, init1;     // initial single-qubit state
   int max_bond;
   double abs_cut, rel_cut;
+  // Partition sets (st_part null for a uniform batch): state b belongs to
+  // partition st_part[b] of width part_n[] and gates part_gate_off[k] ..
+  // part_gate_off[k + 1]; n above is then the widest partition (the stride of
+  // sites and bonds) and P the stride of theta rows.
+  const int32_t *st_part;
+  const int32_t *part_n;
+  const int32_t *part_gate_off;
 };
 
 constexpr int EVOLVE_THREADS = 256;
@@ -109,9 +116,12 @@ evolve_kernel(EvolveParams p) {
 
   const int tid = threadIdx.x;
   const int b = blockIdx.x;
-  const int n = p.n;
+  const int part = p.st_part ? p.st_part[b] : 0;
+  const int n = p.st_part ? p.part_n[part] : p.n;
+  const int gate_begin = p.st_part ? p.part_gate_off[part] : 0;
+  const int gate_end = p.st_part ? p.part_gate_off[part + 1] : p.ngates;
   const double *theta_b = p.theta + (size_t)b * p.P;
-  cplx *sites_b = p.sites + (size_t)b * n * SITE_ELEMS;
+  cplx *sites_b = p.sites + (size_t)b * p.n * SITE_ELEMS;
 
   // |init>^n product state, zero padded; identity pending matrices.
   for (int e = tid; e < n * SITE_ELEMS; e += EVOLVE_THREADS) {
@@ -130,7 +140,7 @@ evolve_kernel(EvolveParams p) {
   __syncthreads();
 
   const double eps = 2.2204460492503131e-16;
-  for (int gi = 0; gi < p.ngates; ++gi) {
+  for (int gi = gate_begin; gi < gate_end; ++gi) {
     const DevGate g = p.gates[gi];
     if (g.kind == GATE_ONE) {
       if (tid == 0) {
@@ -406,7 +416,7 @@ evolve_kernel(EvolveParams p) {
       }
     }
   }
-  for (int s = tid; s <= n; s += EVOLVE_THREADS) p.bonds[(size_t)b * (n + 1) + s] = BOND[s];
+  for (int s = tid; s <= n; s += EVOLVE_THREADS) p.bonds[(size_t)b * (p.n + 1) + s] = BOND[s];
   if (tid == 0) p.status[b] = status;
 }
 

@@ -45,16 +45,12 @@ struct DevNode {    // one trie node
 // ---------------------------------------------------------------------------
 constexpr int RIGHT_THREADS = 256;
 
-__global__ void __launch_bounds__(RIGHT_THREADS)
-right_env_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right,
-                 cplx *__restrict__ branch, const int32_t *__restrict__ status,
-                 double *__restrict__ leafval, int nleaf_total, int identity_leaf) {
+__device__ __forceinline__ void right_env_body(const cplx *__restrict__ sb, int n, cplx *__restrict__ rb,
+                                               cplx *__restrict__ mbase, bool ok, double *leafslot) {
   __shared__ cplx A[SITE_ELEMS];
   __shared__ cplx R[ENV_ELEMS];
   __shared__ cplx T[2 * ENV_ELEMS];
-  const int b = blockIdx.x, tid = threadIdx.x;
-  const cplx *sb = sites + (size_t)b * n * SITE_ELEMS;
-  cplx *rb = right + (size_t)b * (n + 1) * ENV_ELEMS;
+  const int tid = threadIdx.x;
   R[tid] = cmake(tid == 0 ? 1.0 : 0.0, 0.0);
   rb[(size_t)n * ENV_ELEMS + tid] = R[tid];
   for (int s = n - 1; s >= 0; --s) {
@@ -85,16 +81,41 @@ right_env_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right
       const cplx acc = cadd(m0, m1);
       R[tid] = acc;
       rb[(size_t)s * ENV_ELEMS + tid] = acc;
-      if (branch != nullptr) {
-        cplx *mb = branch + ((size_t)b * n + s) * 2 * ENV_ELEMS;
+      if (mbase != nullptr) {
+        cplx *mb = mbase + (size_t)s * 2 * ENV_ELEMS;
         mb[tid] = m0;
         mb[ENV_ELEMS + tid] = m1;
       }
     }
     __syncthreads();
   }
-  if (identity_leaf >= 0 && tid == 0)
-    leafval[(size_t)b * nleaf_total + identity_leaf] = status[b] == 0 ? R[0].x : 0.0;
+  if (leafslot != nullptr && tid == 0) *leafslot = ok ? R[0].x : 0.0;
+}
+
+__global__ void __launch_bounds__(RIGHT_THREADS)
+right_env_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right,
+                 cplx *__restrict__ branch, const int32_t *__restrict__ status,
+                 double *__restrict__ leafval, int nleaf_total, int identity_leaf) {
+  const int b = blockIdx.x;
+  right_env_body(sites + (size_t)b * n * SITE_ELEMS, n, right + (size_t)b * (n + 1) * ENV_ELEMS,
+                 branch ? branch + (size_t)b * n * 2 * ENV_ELEMS : nullptr, status[b] == 0,
+                 identity_leaf >= 0 ? leafval + (size_t)b * nleaf_total + identity_leaf : nullptr);
+}
+
+// Partition sets: state b belongs to partition st_part[b] of width part_n[]
+// (sites / right / branch strides follow the widest partition, n_max) and
+// identity leaf part_idleaf[] (-1 if none).
+__global__ void __launch_bounds__(RIGHT_THREADS)
+right_env_multi_kernel(const cplx *__restrict__ sites, int n_max, const int32_t *__restrict__ st_part,
+                       const int32_t *__restrict__ part_n, const int32_t *__restrict__ part_idleaf,
+                       cplx *__restrict__ right, cplx *__restrict__ branch, const int32_t *__restrict__ status,
+                       double *__restrict__ leafval, int leaf_stride) {
+  const int b = blockIdx.x;
+  const int k = st_part[b];
+  const int idl = part_idleaf[k];
+  right_env_body(sites + (size_t)b * n_max * SITE_ELEMS, part_n[k], right + (size_t)b * (n_max + 1) * ENV_ELEMS,
+                 branch ? branch + (size_t)b * n_max * 2 * ENV_ELEMS : nullptr, status[b] == 0,
+                 (leafval && idl >= 0) ? leafval + (size_t)b * leaf_stride + idl : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -112,6 +133,9 @@ struct LevelParams {
   double *leafval;          // B x nleaf_total
   int ngroups, nslot_prev, nslot_cur, nleaf_total;
   int n, s;
+  // Uneven batches: work items (state, first group, group count) of this level,
+  // three ints each, one per CTA (null: state = blockIdx.y, all groups).
+  const int32_t *work;
 };
 
 struct LevelSmem {
@@ -416,14 +440,11 @@ level_pf_kernel(LevelParams p, int groups_per_warp) {
 // ---------------------------------------------------------------------------
 constexpr int REDUCE_THREADS = 256;
 
-__global__ void __launch_bounds__(REDUCE_THREADS)
-reduce_kernel(const double *__restrict__ leafval, const double *__restrict__ coef, int nleaf,
-              const int32_t *__restrict__ term_leaf, int T, const int32_t *__restrict__ status,
-              double *__restrict__ energies, double *__restrict__ per_term) {
+__device__ __forceinline__ void reduce_body(const double *__restrict__ lv, const double *__restrict__ coef,
+                                            int nleaf, const int32_t *__restrict__ term_leaf, int T, bool ok,
+                                            double *__restrict__ energy, double *__restrict__ per_term) {
   __shared__ double part[REDUCE_THREADS];
-  const int b = blockIdx.x, tid = threadIdx.x;
-  const double *lv = leafval + (size_t)b * nleaf;
-  const bool ok = status[b] == 0;
+  const int tid = threadIdx.x;
   double acc = 0.0;
   for (int i = tid; i < nleaf; i += REDUCE_THREADS) acc = fma(coef[i], lv[i], acc);
   part[tid] = acc;
@@ -432,11 +453,37 @@ reduce_kernel(const double *__restrict__ leafval, const double *__restrict__ coe
     if (tid < w) part[tid] += part[tid + w];
     __syncthreads();
   }
-  if (tid == 0) energies[b] = ok ? part[0] : __longlong_as_double(0x7ff8000000000000LL);
+  if (tid == 0) *energy = ok ? part[0] : __longlong_as_double(0x7ff8000000000000LL);
   if (per_term != nullptr) {
     for (int t = tid; t < T; t += REDUCE_THREADS)
-      per_term[(size_t)b * T + t] = ok ? lv[term_leaf[t]] : __longlong_as_double(0x7ff8000000000000LL);
+      per_term[t] = ok ? lv[term_leaf[t]] : __longlong_as_double(0x7ff8000000000000LL);
   }
+}
+
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_kernel(const double *__restrict__ leafval, const double *__restrict__ coef, int nleaf,
+              const int32_t *__restrict__ term_leaf, int T, const int32_t *__restrict__ status,
+              double *__restrict__ energies, double *__restrict__ per_term) {
+  const int b = blockIdx.x;
+  reduce_body(leafval + (size_t)b * nleaf, coef, nleaf, term_leaf, T, status[b] == 0, energies + b,
+              per_term ? per_term + (size_t)b * T : nullptr);
+}
+
+// Partition sets: partition k = st_part[b] has part_nleaf[k] leaves and
+// part_T[k] terms; its leaf coefficients and term -> leaf map sit at
+// k * leaf_stride and k * term_stride, the state's leaf values and per-term
+// outputs at b * leaf_stride and b * term_stride.
+__global__ void __launch_bounds__(REDUCE_THREADS)
+reduce_multi_kernel(const double *__restrict__ leafval, const double *__restrict__ coef, int leaf_stride,
+                    const int32_t *__restrict__ term_leaf, int term_stride, const int32_t *__restrict__ st_part,
+                    const int32_t *__restrict__ part_nleaf, const int32_t *__restrict__ part_T,
+                    const int32_t *__restrict__ status, double *__restrict__ energies,
+                    double *__restrict__ per_term) {
+  const int b = blockIdx.x;
+  const int k = st_part[b];
+  reduce_body(leafval + (size_t)b * leaf_stride, coef + (size_t)k * leaf_stride, part_nleaf[k],
+              term_leaf + (size_t)k * term_stride, part_T[k], status[b] == 0, energies + b,
+              per_term ? per_term + (size_t)b * term_stride : nullptr);
 }
 
 }  // namespace vqemps

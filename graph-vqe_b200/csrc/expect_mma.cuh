@@ -221,8 +221,22 @@ __global__ void __launch_bounds__(MPF_WARPS * 32, 3)
 level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LevelMmaPfSmem &sm = *reinterpret_cast<LevelMmaPfSmem *>(smem_raw);
-  const int b = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // uniform batch: state blockIdx.y, groups interleaved over the grid;
+  // work list: state w[0], groups w[1] .. w[1] + w[2] split over the warps
+  int b, stride, first, count = 0;
+  if (p.work != nullptr) {
+    const int32_t *w = p.work + 3 * blockIdx.x;
+    b = w[0];
+    stride = MPF_WARPS;
+    first = w[1] + warp;
+    if (warp < w[2]) count = (w[2] - warp + MPF_WARPS - 1) / MPF_WARPS;
+  } else {
+    b = blockIdx.y;
+    stride = gridDim.x * MPF_WARPS;
+    first = blockIdx.x * MPF_WARPS + warp;
+    if (first < p.ngroups) count = min(groups_per_warp, (p.ngroups - first + stride - 1) / stride);
+  }
   {
     const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
     const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
@@ -235,10 +249,6 @@ level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
   cplx *E = sm.E[warp];
   cplx *S = sm.S[warp];
   const int g = lane >> 2, t = lane & 3;
-  const int stride = gridDim.x * MPF_WARPS;
-  const int first = blockIdx.x * MPF_WARPS + warp;
-  int count = 0;
-  if (first < p.ngroups) count = min(groups_per_warp, (p.ngroups - first + stride - 1) / stride);
   if (count == 0) return;
   stage_parent_padded(p, b, first, E, lane);
   cp_async_commit();

@@ -76,6 +76,9 @@ struct SampleParams {
   const int32_t *last_site; // per listed word: last site to sample (inclusive)
   int nwords;
   int32_t *sums;            // B x nwords
+  // partition sets (null: uniform batch): width part_n[st_part[b]], stride n
+  const int32_t *st_part;
+  const int32_t *part_n;
 };
 
 // One thread = one shot. MODE 0: shared sample set, writes packed bits.
@@ -91,7 +94,8 @@ sample_kernel(SampleParams p) {
   const int shot = blockIdx.x * SAMPLE_THREADS + threadIdx.x;
   const bool live = shot < p.shots && p.status[b] == 0;
   const uint64_t seed = MODE == 0 ? p.seeds[b] : p.seeds[(size_t)b * p.nwords + widx];
-  const int last = MODE == 0 ? p.n - 1 : p.last_site[widx];
+  const int nb = p.st_part ? p.part_n[p.st_part[b]] : p.n;
+  const int last = MODE == 0 ? nb - 1 : p.last_site[widx];
   const cplx *sb = p.sites + (size_t)b * p.n * SITE_ELEMS;
 
   cplx v[CHI];
@@ -138,7 +142,7 @@ sample_kernel(SampleParams p) {
       for (int c = 0; c < CHI; ++c) cfma(w[c], v[a], A[(a * 2 + sel) * CHI + c]);
 #pragma unroll
     for (int c = 0; c < CHI; ++c) v[c] = cscale(w[c], inv);
-    const int q = p.site_order == 1 ? p.n - 1 - s : s;
+    const int q = p.site_order == 1 ? nb - 1 - s : s;
     if (sel) word[q >> 6] |= (1ULL << (q & 63));
   }
   if (MODE == 0) {
@@ -192,23 +196,54 @@ zsum_kernel(const uint64_t *__restrict__ bits, int shots, int W, const uint64_t 
   if (t < T) sums[(size_t)b * T + t] = acc;
 }
 
+// Partition sets: state b uses the part_T[k] masks of partition k = st_part[b]
+// (zmask rows k * term_stride ..) and writes sums[b * term_stride + t].
+__global__ void __launch_bounds__(ZSUM_THREADS)
+zsum_multi_kernel(const uint64_t *__restrict__ bits, int shots, int W, const uint64_t *__restrict__ zmask,
+                  int term_stride, const int32_t *__restrict__ st_part, const int32_t *__restrict__ part_T,
+                  int32_t *__restrict__ sums) {
+  __shared__ uint64_t sh[ZSUM_CHUNK * MAX_WORDS64];
+  const int b = blockIdx.y;
+  const int k = st_part[b];
+  const int T = part_T[k];
+  if (blockIdx.x * ZSUM_THREADS >= T) return;
+  const int t = blockIdx.x * ZSUM_THREADS + threadIdx.x;
+  uint64_t m[MAX_WORDS64] = {0, 0, 0, 0};
+  if (t < T)
+    for (int w = 0; w < W; ++w) m[w] = zmask[((size_t)k * term_stride + t) * W + w];
+  int acc = 0;
+  const uint64_t *bb = bits + (size_t)b * shots * W;
+  for (int base = 0; base < shots; base += ZSUM_CHUNK) {
+    const int cnt = min(ZSUM_CHUNK, shots - base);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt * W; e += ZSUM_THREADS) sh[e] = bb[(size_t)base * W + e];
+    __syncthreads();
+    if (t < T) {
+      for (int kk = 0; kk < cnt; ++kk) {
+        int par = 0;
+        for (int w = 0; w < W; ++w) par ^= __popcll(sh[kk * W + w] & m[w]);
+        acc += (par & 1) ? -1 : 1;
+      }
+    }
+  }
+  if (t < T) sums[(size_t)b * term_stride + t] = acc;
+}
+
 // Shot-estimated energies: value_t = sums[t] / shots for sampled words, the
 // analytic per-term value for the others; fixed-order reduction per state.
-__global__ void __launch_bounds__(REDUCE_THREADS)
-sampled_energy_kernel(const int32_t *__restrict__ sums, int sums_stride, const int32_t *__restrict__ sum_index,
-                      const double *__restrict__ analytic, const double *__restrict__ coeffs, int T, int shots,
-                      const int32_t *__restrict__ status, double *__restrict__ energies,
-                      double *__restrict__ per_term) {
+__device__ __forceinline__ void sampled_energy_body(const int32_t *__restrict__ sums,
+                                                    const int32_t *__restrict__ sum_index,
+                                                    const double *__restrict__ analytic,
+                                                    const double *__restrict__ coeffs, int T, int shots, bool ok,
+                                                    double *__restrict__ energy, double *__restrict__ per_term) {
   __shared__ double part[REDUCE_THREADS];
-  const int b = blockIdx.x, tid = threadIdx.x;
-  const bool ok = status[b] == 0;
+  const int tid = threadIdx.x;
   double acc = 0.0;
   for (int t = tid; t < T; t += REDUCE_THREADS) {
     const int si = sum_index[t];
     // si >= 0: sampled word; -2: identity word (+1 on every shot); -1: analytic (X/Y)
-    const double v = si >= 0 ? (double)sums[(size_t)b * sums_stride + si] / shots
-                             : (si == -2 ? 1.0 : analytic[(size_t)b * T + t]);
-    if (per_term) per_term[(size_t)b * T + t] = ok ? v : __longlong_as_double(0x7ff8000000000000LL);
+    const double v = si >= 0 ? (double)sums[si] / shots : (si == -2 ? 1.0 : analytic[t]);
+    if (per_term) per_term[t] = ok ? v : __longlong_as_double(0x7ff8000000000000LL);
     acc = fma(coeffs[t], v, acc);
   }
   part[tid] = acc;
@@ -217,7 +252,33 @@ sampled_energy_kernel(const int32_t *__restrict__ sums, int sums_stride, const i
     if (tid < w) part[tid] += part[tid + w];
     __syncthreads();
   }
-  if (tid == 0) energies[b] = ok ? part[0] : __longlong_as_double(0x7ff8000000000000LL);
+  if (tid == 0) *energy = ok ? part[0] : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+__global__ void __launch_bounds__(REDUCE_THREADS)
+sampled_energy_kernel(const int32_t *__restrict__ sums, int sums_stride, const int32_t *__restrict__ sum_index,
+                      const double *__restrict__ analytic, const double *__restrict__ coeffs, int T, int shots,
+                      const int32_t *__restrict__ status, double *__restrict__ energies,
+                      double *__restrict__ per_term) {
+  const int b = blockIdx.x;
+  sampled_energy_body(sums + (size_t)b * sums_stride, sum_index, analytic ? analytic + (size_t)b * T : nullptr,
+                      coeffs, T, shots, status[b] == 0, energies + b,
+                      per_term ? per_term + (size_t)b * T : nullptr);
+}
+
+// Partition sets: every array is strided by term_stride, per partition
+// (sum_index, coeffs) or per state (sums, analytic, per_term).
+__global__ void __launch_bounds__(REDUCE_THREADS)
+sampled_energy_multi_kernel(const int32_t *__restrict__ sums, const int32_t *__restrict__ sum_index,
+                            const double *__restrict__ analytic, const double *__restrict__ coeffs,
+                            int term_stride, const int32_t *__restrict__ st_part,
+                            const int32_t *__restrict__ part_T, int shots, const int32_t *__restrict__ status,
+                            double *__restrict__ energies, double *__restrict__ per_term) {
+  const int b = blockIdx.x;
+  const int k = st_part[b];
+  const size_t so = (size_t)b * term_stride, po = (size_t)k * term_stride;
+  sampled_energy_body(sums + so, sum_index + po, analytic ? analytic + so : nullptr, coeffs + po, part_T[k],
+                      shots, status[b] == 0, energies + b, per_term ? per_term + so : nullptr);
 }
 
 }  // namespace vqemps

@@ -6,6 +6,6 @@ sampling run in hand-written sm_100a kernels behind the C ABI of
 include/vqemps.h. Python only moves torch tensors and calls that ABI.
 """
 from ._lib import EngineError
-from .engine import Engine, Hamiltonian, counts, unpack_bits
+from .engine import Engine, Hamiltonian, PartitionSet, counts, unpack_bits
 
-__all__ = ["Engine", "EngineError", "Hamiltonian", "counts", "unpack_bits"]
+__all__ = ["Engine", "EngineError", "Hamiltonian", "PartitionSet", "counts", "unpack_bits"]

@@ -28,7 +28,9 @@ SYMBOLS = (
     "vqemps_batch_status", "vqemps_energy_grad_batch", "vqemps_sample",
     "vqemps_sampled_energy", "vqemps_copy_sites", "vqemps_plan_stats", "vqemps_profile_energy",
     "vqemps_energy_noalloc", "vqemps_set_level_variant", "vqemps_level_variant",
-    "vqemps_set_grad_checkpoint",
+    "vqemps_set_grad_checkpoint", "vqemps_set_partitions", "vqemps_free_partitions",
+    "vqemps_partition_info", "vqemps_partition_bond_dims", "vqemps_partition_energy",
+    "vqemps_partition_sample", "vqemps_partition_sampled_energy",
 )
 
 
@@ -82,6 +84,14 @@ def load():
         "vqemps_set_level_variant": (I, [P, I]),
         "vqemps_set_grad_checkpoint": (I, [P, I]),
         "vqemps_level_variant": (I, [P, I, I, ctypes.POINTER(I)]),
+        "vqemps_set_partitions": (I, [P, I, V, ctypes.POINTER(VqempsOp), V, V, V, ctypes.c_char_p, V, V,
+                                      I, I, ctypes.POINTER(I)]),
+        "vqemps_free_partitions": (I, [P, I]),
+        "vqemps_partition_info": (I, [P, I, V, V, V]),
+        "vqemps_partition_bond_dims": (I, [P, I, I, ctypes.POINTER(I)]),
+        "vqemps_partition_energy": (I, [P, I, V, I, V, V, V]),
+        "vqemps_partition_sample": (I, [P, I, V, I, I, u64, I, V, V]),
+        "vqemps_partition_sampled_energy": (I, [P, I, V, I, I, u64, I, V, V, V, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -94,6 +94,39 @@ def compile_ops(ops, n):
     return arr, len(out), m, len(mats)
 
 
+@dataclass
+class PartitionSet:
+    """Independent circuits of uneven width loaded into an engine together.
+
+    ``ns[k]``/``params[k]``/``T[k]``: qubits, parameters and terms of partition
+    k; parameter rows are ``P_max`` wide and per-term rows ``T_max`` wide;
+    shots pack into ``W`` 64-bit words.
+    """
+    handle: int
+    ns: list
+    params: list
+    T: list
+    n_max: int
+    P_max: int
+    T_max: int
+    W: int
+    levels: int
+    flops: float
+
+    @property
+    def K(self):
+        return len(self.ns)
+
+    def pack_theta(self, thetas, copies: int = 1, device=None):
+        """Per-partition angle arrays -> the [K * copies, P_max] row layout
+        (row k * copies + c; ``thetas[k]`` is [P_k] or [copies, P_k])."""
+        out = torch.zeros((self.K * copies, self.P_max), dtype=torch.float64)
+        for k, th in enumerate(thetas):
+            t = torch.as_tensor(th, dtype=torch.float64).reshape(-1, self.params[k])
+            out[k * copies:(k + 1) * copies, :self.params[k]] = t.expand(copies, -1) if t.shape[0] == 1 else t
+        return out.to(device) if device is not None else out
+
+
 class Engine:
     """One engine context on one CUDA device.
 
@@ -258,6 +291,109 @@ class Engine:
                                                        _ptr(pt), _stream(stream)), "sampled_energy")
         self.check_status(B, stream)
         return (e, pt) if per_term else e
+
+    # -- partition sets ------------------------------------------------------
+    def set_partitions(self, parts, initial=None, site_order: str = "msb") -> PartitionSet:
+        """Load independent problems ``(n, ops, words, coeffs)`` as one partition set."""
+        K = len(parts)
+        ns = np.zeros(K, dtype=np.int32)
+        op_off = np.zeros(K + 1, dtype=np.int32)
+        mat_off = np.zeros(K + 1, dtype=np.int32)
+        term_off = np.zeros(K + 1, dtype=np.int64)
+        all_ops, all_mats, all_words, all_coeffs = [], [], [], []
+        for k, (n, ops, words, coeffs) in enumerate(parts):
+            arr, count, mats, nm = compile_ops(ops, n)
+            words = list(words)
+            if len(words) != len(coeffs):
+                raise EngineError(_lib.INVALID, "words and coefficients differ in length")
+            for w in words:
+                if len(w) != n:
+                    raise EngineError(_lib.INVALID, "Invalid analytic Pauli width")
+            ns[k] = n
+            all_ops.extend(arr[i] for i in range(count))
+            all_mats.append(mats[:2 * nm])
+            all_words.append("".join(words))
+            all_coeffs.append(np.asarray(coeffs, dtype=np.float64))
+            op_off[k + 1] = op_off[k] + count
+            mat_off[k + 1] = mat_off[k] + nm
+            term_off[k + 1] = term_off[k] + len(words)
+        ops_arr = (VqempsOp * max(len(all_ops), 1))(*all_ops)
+        mats = np.ascontiguousarray(np.concatenate(all_mats + [np.zeros(2)]))
+        coeffs = np.ascontiguousarray(np.concatenate(all_coeffs + [np.zeros(1)]))
+        buf = "".join(all_words).encode("ascii")
+        order = {"qubit": 0, "msb": 1}[site_order]
+        h = ctypes.c_int()
+        vp = lambda a: ctypes.c_void_p(a.ctypes.data)
+        check(self.ctx, self.lib.vqemps_set_partitions(
+            self.ctx, K, vp(ns), ops_arr, vp(op_off), vp(mats), vp(mat_off), buf, vp(term_off), vp(coeffs),
+            _lib.INITIAL[initial], order, ctypes.byref(h)), "set_partitions")
+        info = np.zeros(6, dtype=np.int32)
+        params = np.zeros(K, dtype=np.int32)
+        flops = ctypes.c_double()
+        check(self.ctx, self.lib.vqemps_partition_info(self.ctx, h.value, vp(info), vp(params),
+                                                       ctypes.byref(flops)), "partition_info")
+        return PartitionSet(h.value, ns.tolist(), params.tolist(), np.diff(term_off).tolist(),
+                            int(info[1]), int(info[2]), int(info[3]), int(info[4]), int(info[5]),
+                            flops.value)
+
+    def free_partitions(self, pset: PartitionSet):
+        check(self.ctx, self.lib.vqemps_free_partitions(self.ctx, pset.handle), "free_partitions")
+
+    def partition_bond_dims(self, pset: PartitionSet, k: int):
+        dims = (ctypes.c_int * (pset.ns[k] + 1))()
+        check(self.ctx, self.lib.vqemps_partition_bond_dims(self.ctx, pset.handle, k, dims), "partition_bond_dims")
+        return list(dims)
+
+    def _part_theta(self, pset: PartitionSet, theta, copies: int):
+        t = torch.as_tensor(theta, dtype=torch.float64, device=self.device)
+        if t.dim() != 2 or t.shape[0] != pset.K * copies or t.shape[1] != pset.P_max:
+            raise EngineError(_lib.INVALID, f"expected theta of shape [{pset.K * copies}, {pset.P_max}]")
+        return t.contiguous()
+
+    def partition_energy(self, pset: PartitionSet, theta, copies: int = 1, per_term: bool = False,
+                         stream=None, check_status: bool = True):
+        """Energies of ``copies`` parameter sets of every partition (state k * copies + c)."""
+        t = self._part_theta(pset, theta, copies)
+        B = pset.K * copies
+        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        pt = torch.empty((B, pset.T_max), dtype=torch.float64, device=self.device) if per_term else None
+        check(self.ctx, self.lib.vqemps_partition_energy(self.ctx, pset.handle, _ptr(t), copies, _ptr(e),
+                                                         _ptr(pt), _stream(stream)), "partition_energy")
+        if check_status:
+            self.check_status(B, stream)
+        return (e, pt) if per_term else e
+
+    def partition_sample(self, pset: PartitionSet, theta, shots: int, seed: int, rng: str = "philox",
+                         copies: int = 1, stream=None):
+        """Packed bitstrings [K * copies, shots, W] (bit q = qubit q of the state's partition)."""
+        t = self._part_theta(pset, theta, copies)
+        B = pset.K * copies
+        bits = torch.empty((B, shots, pset.W), dtype=torch.int64, device=self.device)
+        check(self.ctx, self.lib.vqemps_partition_sample(self.ctx, pset.handle, _ptr(t), copies, shots, seed,
+                                                         _lib.RNG[rng], _ptr(bits), _stream(stream)),
+              "partition_sample")
+        self.check_status(B, stream)
+        return bits
+
+    def partition_sampled_energy(self, pset: PartitionSet, theta, shots: int, seed: int, rng: str = "philox",
+                                 copies: int = 1, per_term: bool = False, return_bits: bool = False,
+                                 stream=None):
+        """Shot-estimated energies (one shared sample set per state), optionally the shots."""
+        t = self._part_theta(pset, theta, copies)
+        B = pset.K * copies
+        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        pt = torch.empty((B, pset.T_max), dtype=torch.float64, device=self.device) if per_term else None
+        bits = torch.empty((B, shots, pset.W), dtype=torch.int64, device=self.device) if return_bits else None
+        check(self.ctx, self.lib.vqemps_partition_sampled_energy(
+            self.ctx, pset.handle, _ptr(t), copies, shots, seed, _lib.RNG[rng], _ptr(e), _ptr(pt), _ptr(bits),
+            _stream(stream)), "partition_sampled_energy")
+        self.check_status(B, stream)
+        out = [e]
+        if per_term:
+            out.append(pt)
+        if return_bits:
+            out.append(bits)
+        return tuple(out) if len(out) > 1 else e
 
     def sites(self, b: int = 0, stream=None) -> np.ndarray:
         """Padded site tensors [n, 16, 2, 16] of state b of the last batch."""

@@ -199,6 +199,47 @@ int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats);
  * Used to check the prepared state against the oracle (synchronises). */
 int vqemps_copy_sites(vqemps_ctx *ctx, int b, double *sites_host, void *stream);
 
+/* Partition sets: K independent circuits of uneven width, parameter count and
+ * Hamiltonian evaluated in one batch. Replaces the plain partition warm start's
+ * sequential local solves, one observe() per energy and partition
+ * (test/sources/independent-vqe/Qiskit_VQE/independent_vqe.py:276-290 ->
+ * test/tools/independent_campaign.py:15-63 _minimize_model). Partition k has
+ * ns[k] qubits, ops[op_off[k] .. op_off[k+1]) (matrix indices relative to
+ * matrices + 2 * matrix_off[k], matrix_off may be NULL), and the Pauli sum of
+ * rows term_off[k] .. term_off[k+1] of coeffs, whose words are packed one
+ * partition after another, each ns[k] characters wide (qubit order, as
+ * vqemps_set_hamiltonian). Every partition compiles exactly as a one-circuit
+ * engine would; initial state and site order are shared. */
+int vqemps_set_partitions(vqemps_ctx *ctx, int K, const int32_t *ns, const vqemps_op *ops,
+                          const int32_t *op_off, const double *matrices, const int32_t *matrix_off,
+                          const char *words, const int64_t *term_off, const double *coeffs,
+                          int initial, int site_order, int *handle);
+int vqemps_free_partitions(vqemps_ctx *ctx, int handle);
+/* info[6]: K, widest partition n_max, theta row stride P_max, per-term row
+ * stride T_max, 64-bit words per shot W, trie levels; params[K] (may be NULL):
+ * parameters of each partition; flops (may be NULL): FP64 flops of one
+ * evaluation of every partition. */
+int vqemps_partition_info(vqemps_ctx *ctx, int handle, int32_t *info, int32_t *params, double *flops);
+/* Allocation bounds of partition k (ns[k] + 1 entries). */
+int vqemps_partition_bond_dims(vqemps_ctx *ctx, int handle, int k, int *dims);
+/* Analytic energies of copies parameter sets of every partition: state
+ * b = k * copies + c; theta_dev (K * copies) x P_max (partition k reads the
+ * first P_k entries of its rows), energies_dev K * copies, per_term_dev
+ * (optional) (K * copies) x T_max. Status per state: vqemps_batch_status. */
+int vqemps_partition_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int copies,
+                            double *energies_dev, double *per_term_dev, void *stream);
+/* Bitstrings of every state: packed_dev (K * copies) x shots x W, bit q of a
+ * shot is qubit q of its partition; state b uses evaluation seed seed + b, as
+ * vqemps_sample. */
+int vqemps_partition_sample(vqemps_ctx *ctx, int handle, const double *theta_dev, int copies, int shots,
+                            uint64_t seed, int rng, uint64_t *packed_dev, void *stream);
+/* Shot-estimated energies from one shared sample set per state (I/Z words from
+ * the shots, X/Y words analytic: VQEMPS_SHOTS_SHARED semantics). packed_dev
+ * (optional) receives the shots as vqemps_partition_sample writes them. */
+int vqemps_partition_sampled_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int copies,
+                                    int shots, uint64_t seed, int rng, double *energies_dev,
+                                    double *per_term_dev, uint64_t *packed_dev, void *stream);
+
 /* Allocation-free analytic energy of ONE parameter set. No counterpart in the
  * reference: it exists for callers that must not allocate device memory while
  * they run -- for example a simulator plugin hosted inside a runtime that owns
