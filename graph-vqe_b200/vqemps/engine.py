@@ -233,11 +233,12 @@ class Engine:
 
     # -- analytic energies ---------------------------------------------------
     def energy(self, ham: Hamiltonian, theta, per_term: bool = False, stream=None,
-               check_status: bool = True):
-        """Energies of B parameter sets (device tensors); optionally <P_k> per term."""
+               check_status: bool = True, out=None):
+        """Energies of B parameter sets (device tensors); optionally <P_k> per term.
+        ``out`` (a [B] float64 device tensor) receives the energies in place."""
         t = self._theta(theta)
         B = t.shape[0]
-        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        e = out if out is not None else torch.empty(B, dtype=torch.float64, device=self.device)
         pt = torch.empty((B, ham.T), dtype=torch.float64, device=self.device) if per_term else None
         check(self.ctx, self.lib.vqemps_energy_batch(self.ctx, ham.handle, _ptr(t), B, _ptr(e), _ptr(pt),
                                                      _stream(stream)), "energy_batch")
@@ -267,6 +268,27 @@ class Engine:
         check(self.ctx, self.lib.vqemps_energy_grad_batch(self.ctx, ham.handle, _ptr(t), B, _ptr(e),
                                                           _ptr(g), _stream(stream)), "energy_grad_batch")
         return e, g
+
+    def capture(self, fn, warmup: int = 2):
+        """Record ``fn()`` -- engine calls on fixed device tensors, without status
+        checks (they synchronise) -- into a CUDA graph and return it.
+
+        ``fn`` runs ``warmup`` times first on a side stream, so workspaces reach
+        their size and the level-kernel autotuner has decided before capture (a
+        captured call may not allocate or synchronise). ``graph.replay()`` then
+        re-runs every launch of the call with one submission; write new angles
+        into the captured theta tensor in place between replays."""
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                fn()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            fn()
+        return graph
 
     # -- sampling ------------------------------------------------------------
     def sample(self, theta, shots: int, seed: int, rng: str = "splitmix", stream=None):
@@ -351,11 +373,11 @@ class Engine:
         return t.contiguous()
 
     def partition_energy(self, pset: PartitionSet, theta, copies: int = 1, per_term: bool = False,
-                         stream=None, check_status: bool = True):
+                         stream=None, check_status: bool = True, out=None):
         """Energies of ``copies`` parameter sets of every partition (state k * copies + c)."""
         t = self._part_theta(pset, theta, copies)
         B = pset.K * copies
-        e = torch.empty(B, dtype=torch.float64, device=self.device)
+        e = out if out is not None else torch.empty(B, dtype=torch.float64, device=self.device)
         pt = torch.empty((B, pset.T_max), dtype=torch.float64, device=self.device) if per_term else None
         check(self.ctx, self.lib.vqemps_partition_energy(self.ctx, pset.handle, _ptr(t), copies, _ptr(e),
                                                          _ptr(pt), _stream(stream)), "partition_energy")
