@@ -31,6 +31,9 @@ SYMBOLS = (
     "vqemps_set_grad_checkpoint", "vqemps_set_partitions", "vqemps_free_partitions",
     "vqemps_partition_info", "vqemps_partition_bond_dims", "vqemps_partition_energy",
     "vqemps_partition_sample", "vqemps_partition_sampled_energy",
+    "vqemps_mpnn_create", "vqemps_mpnn_destroy", "vqemps_mpnn_last_error", "vqemps_mpnn_num_params",
+    "vqemps_mpnn_set_params", "vqemps_mpnn_get_params", "vqemps_mpnn_forward", "vqemps_mpnn_loss",
+    "vqemps_mpnn_backward", "vqemps_mpnn_adam_step",
 )
 
 
@@ -38,6 +41,13 @@ class VqempsOp(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("q0", ctypes.c_int32), ("q1", ctypes.c_int32),
                 ("param", ctypes.c_int32), ("angle", ctypes.c_double),
                 ("matrix", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class VqempsGraph(ctypes.Structure):
+    _fields_ = [("num_nodes", ctypes.c_int32), ("num_edges", ctypes.c_int32),
+                ("node_feat", ctypes.c_void_p), ("edge_feat", ctypes.c_void_p),
+                ("edge_src", ctypes.c_void_p), ("edge_dst", ctypes.c_void_p),
+                ("dst_off", ctypes.c_void_p), ("src_perm", ctypes.c_void_p), ("src_off", ctypes.c_void_p)]
 
 
 class EngineError(RuntimeError):
@@ -92,6 +102,17 @@ def load():
         "vqemps_partition_energy": (I, [P, I, V, I, V, V, V]),
         "vqemps_partition_sample": (I, [P, I, V, I, I, u64, I, V, V]),
         "vqemps_partition_sampled_energy": (I, [P, I, V, I, I, u64, I, V, V, V, V]),
+        "vqemps_mpnn_create": (I, [I, I, I, I, I, I, ctypes.POINTER(P)]),
+        "vqemps_mpnn_destroy": (I, [P]),
+        "vqemps_mpnn_last_error": (ctypes.c_char_p, [P]),
+        "vqemps_mpnn_num_params": (I, [P, ctypes.POINTER(ctypes.c_int64)]),
+        "vqemps_mpnn_set_params": (I, [P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64]),
+        "vqemps_mpnn_get_params": (I, [P, ctypes.POINTER(ctypes.c_float), ctypes.c_int64]),
+        "vqemps_mpnn_forward": (I, [P, ctypes.POINTER(VqempsGraph), V, V]),
+        "vqemps_mpnn_loss": (I, [P, V, V, V, V, V]),
+        "vqemps_mpnn_backward": (I, [P, ctypes.POINTER(VqempsGraph), V, V, V]),
+        "vqemps_mpnn_adam_step": (I, [P, V, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                      ctypes.c_float, V]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -20,7 +20,7 @@ NVCC_FLAGS = [
 
 def sources():
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + \
-        [ROOT / "include" / "vqemps.h"]
+        sorted((ROOT / "include").glob("*.h"))
 
 
 def needs_build() -> bool:
@@ -34,7 +34,9 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, str(CSRC / "engine.cu"), "-o", str(OUT)]
+    # engine.cu includes the other engine sources; mpnn.cu (the warm-start
+    # network) is its own translation unit in the same library
+    cmd = [nvcc, *NVCC_FLAGS, str(CSRC / "engine.cu"), str(CSRC / "mpnn.cu"), "-o", str(OUT)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     res = subprocess.run(cmd, capture_output=True, text=True)

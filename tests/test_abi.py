@@ -1,5 +1,5 @@
 """The C-ABI library builds for sm_100a, loads without a GPU and exports every
-entry point that include/vqemps.h declares (no compute calls here)."""
+entry point that include/*.h declares (no compute calls here)."""
 import ctypes
 import re
 from pathlib import Path
@@ -8,7 +8,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def declared_symbols():
-    text = (ROOT / "include" / "vqemps.h").read_text()
+    text = "\n".join(p.read_text() for p in sorted((ROOT / "include").glob("*.h")))
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(vqemps_[a-z_0-9]+)\s*\(", text)))
 
@@ -32,6 +32,8 @@ def test_binding_loads_and_rejects_bad_arguments_without_a_gpu():
     assert lib.vqemps_create(0, 16, -1.0, 0.0, ctypes.byref(ctypes.c_void_p())) == _lib.INVALID
     assert lib.vqemps_last_error(None) == b"null context"
     assert lib.vqemps_destroy(None) == _lib.OK
+    assert lib.vqemps_mpnn_create(0, 4, 3, 100, 3, 5, ctypes.byref(ctypes.c_void_p())) == _lib.INVALID
+    assert lib.vqemps_mpnn_last_error(None) == b"null network"
 
 
 def test_built_for_sm_100a():
