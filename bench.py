@@ -218,7 +218,7 @@ def main():
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     import vqemps
-    from oracle import workloads as W
+    from vqemps import workloads as W
 
     spec, words, coeffs, thetas = W.batched_40q(seed=0, batch=args.batch)
     # each rank gets its own probe set: shift the SPSA center per rank

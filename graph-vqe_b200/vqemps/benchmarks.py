@@ -26,7 +26,7 @@ for _p in (ROOT, ROOT / "graph-vqe_b200"):
         sys.path.insert(0, str(_p))
 
 import vqemps  # noqa: E402
-from oracle import workloads as W  # noqa: E402
+from vqemps import workloads as W  # noqa: E402
 
 
 def _events_ms(fn, reps, stream):

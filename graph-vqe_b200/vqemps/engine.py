@@ -198,6 +198,9 @@ class Engine:
             len(words), ctypes.byref(h)), "set_hamiltonian")
         return Hamiltonian(h.value, self.n, len(words), words, coeffs)
 
+    def free_hamiltonian(self, ham: Hamiltonian):
+        check(self.ctx, self.lib.vqemps_free_hamiltonian(self.ctx, ham.handle), "free_hamiltonian")
+
     LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf")
 
     def set_level_variant(self, variant):

@@ -142,6 +142,89 @@ class _RoundBatcher:
                 self.cv.notify_all()
 
 
+def minimize_model(params, maxiter, constant, energies, value_grad, *, energy_tol=1.0,
+                   use_gradient_optimizer=True):
+    """One model's optimisation (independent_vqe.py:176-245).
+
+    ``energies(X)`` -> energies of the rows of X; ``value_grad(x)`` -> (E, dE/dx),
+    or None to use the parameter-shift rule through ``energies``."""
+    params = np.asarray(params, dtype=float).copy()
+    cache = {}
+    grads = {}
+    best = [float("inf"), params.copy()]
+    previous = [None]
+    accepted = [0]
+    reason = ["iteration_limit"]
+    history = []
+
+    def record(x, e):
+        cache[np.asarray(x).tobytes()] = e
+        if previous[0] is None:
+            previous[0] = e
+        if e < best[0]:
+            best[:] = [e, np.asarray(x).copy()]
+        history.append(e)
+
+    def evaluate_with_gradient(x):
+        if value_grad is not None:
+            e, g = value_grad(x)
+        else:
+            P = x.size
+            shifted = np.repeat(x[None, :], 2 * P + 1, axis=0)
+            idx = np.arange(P)
+            shifted[1 + idx, idx] += np.pi / 2
+            shifted[1 + P + idx, idx] -= np.pi / 2
+            v = energies(shifted)
+            e, g = v[0], (v[1:P + 1] - v[P + 1:]) / 2
+        grads[np.asarray(x).tobytes()] = np.asarray(g, dtype=float)
+        return float(e)
+
+    def cost(x):
+        key = np.asarray(x).tobytes()
+        if key in cache:
+            return cache[key]
+        e = evaluate_with_gradient(x) if use_gradient_optimizer else float(energies(x[None, :])[0])
+        record(x, e)
+        return e
+
+    def gradient(x):
+        key = np.asarray(x).tobytes()
+        if key not in grads:
+            evaluate_with_gradient(x)
+        return grads[key]
+
+    def callback(*args, **kwargs):
+        x = np.asarray(kwargs.get("intermediate_result").x if "intermediate_result" in kwargs else args[0])
+        key = x.tobytes()
+        e = cache[key] if key in cache else cost(x)
+        improvement = previous[0] - e
+        previous[0] = e
+        accepted[0] += 1
+        cache.clear()
+        cache[key] = e
+        if improvement < energy_tol:
+            reason[0] = "energy_improvement_below_threshold"
+            raise EarlyStop()
+
+    started = time.perf_counter()
+    cost(params)
+    if maxiter and not constant:
+        try:
+            if use_gradient_optimizer:
+                res = minimize(cost, params, method="L-BFGS-B", jac=gradient, callback=callback,
+                               options=dict(maxiter=maxiter, ftol=1e-12, gtol=1e-8))
+            else:
+                res = minimize(cost, params, method="COBYLA", callback=callback,
+                               options=dict(maxiter=maxiter, tol=1e-8))
+            reason[0] = str(res.message)
+        except EarlyStop:
+            pass
+    elif constant:
+        reason[0] = "constant_local_objective"
+    return dict(energy=float(best[0]), params=best[1], accepted_iterations=accepted[0], stop_reason=reason[0],
+                duration_s=time.perf_counter() - started, history=history)
+
+
 class PartitionPlan:
     """Host-only part of the strategy: simplified Hamiltonian, coupling graph,
     blocks and local models (no GPU needed).
@@ -231,6 +314,41 @@ class PartitionPlan:
                 parameter_indices=np.array([(layer * self.n + q) * G + g for layer in range(self.reps + 1)
                                             for q in block for g in range(G)], dtype=np.int64)))
 
+class GlobalProblem:
+    """The full-width objective on the engine: the nearest-neighbour ansatz over
+    all qubits and the whole Hamiltonian (``_build_kernel([range(n)], ...)``,
+    independent_vqe.py:106-110), with the energy, the adjoint value/gradient and
+    the global refinement."""
+
+    def __init__(self, engine, n, words, coeffs, *, reps=4, su2_gates=("ry",), entanglement="linear",
+                 energy_tol=1.0, use_gradient_optimizer=True):
+        self.engine = engine
+        self.n = n
+        self.energy_tol = energy_tol
+        self.use_gradient_optimizer = use_gradient_optimizer
+        self.ops, self.num_params = ansatz_ops(n, reps, tuple(su2_gates), entanglement)
+        width = max(2, n)
+        engine.set_circuit(width, self.ops, site_order="msb")
+        words = [w + "I" * (width - n) for w in words] or ["I" * width]
+        self.ham = engine.set_hamiltonian(words, coeffs if len(coeffs) else [0.0])
+
+    def energy(self, theta):
+        import torch
+        t = torch.as_tensor(np.atleast_2d(theta), dtype=torch.float64, device=self.engine.device)
+        return self.engine.energy(self.ham, t).cpu().numpy()
+
+    def value_grad(self, theta):
+        import torch
+        t = torch.as_tensor(np.atleast_2d(theta), dtype=torch.float64, device=self.engine.device)
+        e, g = self.engine.energy_grad(self.ham, t)
+        return float(e[0]), g[0].cpu().numpy()
+
+    def refine(self, theta, maxiter):
+        return minimize_model(theta, maxiter, False, self.energy,
+                              self.value_grad if self.use_gradient_optimizer else None,
+                              energy_tol=self.energy_tol, use_gradient_optimizer=self.use_gradient_optimizer)
+
+
 class IndependentPartitionVQE:
     """Partition warm start + global refinement of one Hamiltonian on one engine.
 
@@ -257,90 +375,9 @@ class IndependentPartitionVQE:
         self.blocks = self.plan.blocks
         self.local_models = self.plan.local_models
         self.num_params = self.plan.num_params
-        width = max(2, n)
-        engine.set_circuit(width, self.plan.global_ops, site_order="msb")
-        words = [w + "I" * (width - n) for w in self.plan.words] or ["I" * width]
-        self.ham = engine.set_hamiltonian(words, self.plan.coeffs if len(self.plan.words) else [0.0])
-
-    # -- one model's optimisation (independent_vqe.py:176-245) ---------------
-    def _minimize_model(self, params, maxiter, constant, energies, value_grad):
-        """``energies(X)`` -> energies of the rows of X; ``value_grad(x)`` ->
-        (E, dE/dx) or None to use the parameter-shift rule through ``energies``."""
-        params = np.asarray(params, dtype=float).copy()
-        cache = {}
-        grads = {}
-        best = [float("inf"), params.copy()]
-        previous = [None]
-        accepted = [0]
-        reason = ["iteration_limit"]
-        history = []
-
-        def record(x, e):
-            cache[np.asarray(x).tobytes()] = e
-            if previous[0] is None:
-                previous[0] = e
-            if e < best[0]:
-                best[:] = [e, np.asarray(x).copy()]
-            history.append(e)
-
-        def evaluate_with_gradient(x):
-            if value_grad is not None:
-                e, g = value_grad(x)
-            else:
-                P = x.size
-                shifted = np.repeat(x[None, :], 2 * P + 1, axis=0)
-                idx = np.arange(P)
-                shifted[1 + idx, idx] += np.pi / 2
-                shifted[1 + P + idx, idx] -= np.pi / 2
-                v = energies(shifted)
-                e, g = v[0], (v[1:P + 1] - v[P + 1:]) / 2
-            grads[np.asarray(x).tobytes()] = np.asarray(g, dtype=float)
-            return float(e)
-
-        def cost(x):
-            key = np.asarray(x).tobytes()
-            if key in cache:
-                return cache[key]
-            e = evaluate_with_gradient(x) if self.use_gradient_optimizer else float(energies(x[None, :])[0])
-            record(x, e)
-            return e
-
-        def gradient(x):
-            key = np.asarray(x).tobytes()
-            if key not in grads:
-                evaluate_with_gradient(x)
-            return grads[key]
-
-        def callback(*args, **kwargs):
-            x = np.asarray(kwargs.get("intermediate_result").x if "intermediate_result" in kwargs else args[0])
-            key = x.tobytes()
-            e = cache[key] if key in cache else cost(x)
-            improvement = previous[0] - e
-            previous[0] = e
-            accepted[0] += 1
-            cache.clear()
-            cache[key] = e
-            if improvement < self.energy_tol:
-                reason[0] = "energy_improvement_below_threshold"
-                raise EarlyStop()
-
-        started = time.perf_counter()
-        cost(params)
-        if maxiter and not constant:
-            try:
-                if self.use_gradient_optimizer:
-                    res = minimize(cost, params, method="L-BFGS-B", jac=gradient, callback=callback,
-                                   options=dict(maxiter=maxiter, ftol=1e-12, gtol=1e-8))
-                else:
-                    res = minimize(cost, params, method="COBYLA", callback=callback,
-                                   options=dict(maxiter=maxiter, tol=1e-8))
-                reason[0] = str(res.message)
-            except EarlyStop:
-                pass
-        elif constant:
-            reason[0] = "constant_local_objective"
-        return dict(energy=float(best[0]), params=best[1], accepted_iterations=accepted[0], stop_reason=reason[0],
-                    duration_s=time.perf_counter() - started, history=history)
+        self.problem = GlobalProblem(engine, n, self.plan.words, self.plan.coeffs, reps=reps, su2_gates=su2_gates,
+                                     entanglement=entanglement, energy_tol=energy_tol,
+                                     use_gradient_optimizer=use_gradient_optimizer)
 
     # -- local phase: all blocks at once ---------------------------------------
     def solve_locals(self, theta):
@@ -356,8 +393,9 @@ class IndependentPartitionVQE:
         def work(k):
             try:
                 m = self.local_models[k]
-                results[k] = self._minimize_model(theta[m["parameter_indices"]], self.block_maxiter, m["constant"],
-                                                  lambda X: batcher.request(k, X), None)
+                results[k] = minimize_model(theta[m["parameter_indices"]], self.block_maxiter, m["constant"],
+                                            lambda X: batcher.request(k, X), None, energy_tol=self.energy_tol,
+                                            use_gradient_optimizer=self.use_gradient_optimizer)
             except BaseException as exc:
                 errors.append(exc)
             finally:
@@ -377,20 +415,14 @@ class IndependentPartitionVQE:
 
     # -- global objective ------------------------------------------------------
     def energy(self, theta):
-        import torch
-        t = torch.as_tensor(np.atleast_2d(theta), dtype=torch.float64, device=self.engine.device)
-        return self.engine.energy(self.ham, t).cpu().numpy()
+        return self.problem.energy(theta)
 
     def value_grad(self, theta):
-        import torch
-        t = torch.as_tensor(np.atleast_2d(theta), dtype=torch.float64, device=self.engine.device)
-        e, g = self.engine.energy_grad(self.ham, t)
-        return float(e[0]), g[0].cpu().numpy()
+        return self.problem.value_grad(theta)
 
     def refine(self, theta, maxiter=None):
         """Global refinement from ``theta`` (the reference's global _minimize_model)."""
-        return self._minimize_model(theta, self.global_maxiter if maxiter is None else maxiter, False,
-                                    self.energy, self.value_grad if self.use_gradient_optimizer else None)
+        return self.problem.refine(theta, self.global_maxiter if maxiter is None else maxiter)
 
     def initial_theta(self):
         return np.random.default_rng(self.seed).uniform(-np.pi, np.pi, self.num_params)

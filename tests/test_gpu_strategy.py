@@ -27,7 +27,7 @@ def _problem(n=20, T=150, seed=2):
 
 
 def test_batched_local_solves_equal_sequential_solves(vq):
-    from vqemps.strategy import IndependentPartitionVQE
+    from vqemps.strategy import IndependentPartitionVQE, minimize_model
     n, words, coeffs = _problem()
     eng = vq.Engine(0, 16)
     strat = IndependentPartitionVQE(eng, n, words, coeffs, block_maxiter=6, max_block_qubits=8)
@@ -40,7 +40,8 @@ def test_batched_local_solves_equal_sequential_solves(vq):
         se.set_level_variant("dmma_pf")
         h = se.set_hamiltonian([t for t, _ in m["terms"]], [c for _, c in m["terms"]])
         energies = lambda X: se.energy(h, torch.as_tensor(X, device=se.device)).cpu().numpy()  # noqa: E731
-        seq = strat._minimize_model(theta[m["parameter_indices"]], 6, m["constant"], energies, None)
+        seq = minimize_model(theta[m["parameter_indices"]], 6, m["constant"], energies, None,
+                             energy_tol=strat.energy_tol)
         assert seq["energy"] == r["energy"]
         assert np.array_equal(seq["params"], r["params"])
         assert seq["history"] == r["history"]
@@ -51,13 +52,13 @@ def test_batched_local_solves_equal_sequential_solves(vq):
 
 
 def test_global_refinement_adjoint_matches_parameter_shift(vq):
-    from vqemps.strategy import IndependentPartitionVQE
+    from vqemps.strategy import IndependentPartitionVQE, minimize_model
     n, words, coeffs = _problem(n=14, T=120, seed=5)
     eng = vq.Engine(0, 16)
     strat = IndependentPartitionVQE(eng, n, words, coeffs, global_maxiter=3, energy_tol=1e-9)
     theta = strat.initial_theta()
     adj = strat.refine(theta)
-    shift = strat._minimize_model(theta, 3, False, strat.energy, None)
+    shift = minimize_model(theta, 3, False, strat.energy, None, energy_tol=strat.energy_tol)
     assert abs(adj["energy"] - shift["energy"]) <= 1e-8 * max(1.0, abs(shift["energy"]))
     assert np.allclose(adj["params"], shift["params"], atol=1e-6)
 
@@ -69,6 +70,6 @@ def test_full_plain_method_run(vq):
     strat = IndependentPartitionVQE(eng, n, words, coeffs, block_maxiter=10, global_maxiter=5)
     out = strat.run()
     assert np.isfinite(out["warm_start_energy"]) and out["best_energy"] <= out["warm_start_energy"]
-    ref = O.reverse_energy(dict(n=n, ops=strat.plan.global_ops, initial=None, count=strat.num_params),
+    ref = O.reverse_energy(dict(n=n, ops=strat.problem.ops, initial=None, count=strat.num_params),
                            strat.plan.words, strat.plan.coeffs, out["best_params"])
     assert abs(ref - out["best_energy"]) <= 1e-9 * max(1.0, abs(ref))

@@ -54,11 +54,14 @@ def test_features_and_batch_layout():
     words = ["ZIII", "IZZI", "XIIX", "ZZII", "IIIZ"]
     coeffs = [2.0, -1.0, 0.5, 3.0, -4.0]
     node, ei, ef = graph_features(4, words, coeffs)
-    assert node.shape == (4, 4) and np.isclose(node[0, 0], np.log1p(2.0)) and np.isclose(node[3, 0], -np.log1p(4.0))
+    assert node.shape == (4, 4) and np.isclose(node[0, 0], np.log1p(2.0) / 5) and np.isclose(node[3, 0], -np.log1p(4.0) / 5)
+    assert np.isclose(node[0, 1], np.log1p(2.0 + 0.5 + 3.0) / 10)
     pairs = {(a, b) for a, b in ei.T}
     assert {(0, 3), (3, 0), (1, 2), (0, 1), (2, 3)} <= pairs
     k = [i for i, (a, b) in enumerate(ei.T) if (a, b) == (0, 1)][0]
-    assert np.isclose(ef[k, 0], np.log1p(3.0)) and ef[k, 2] == 1.0
+    assert np.isclose(ef[k, 0], np.log1p(3.0) / 5) and ef[k, 2] == 1.0
+    k3 = [i for i, (a, b) in enumerate(ei.T) if (a, b) == (3, 0)][0]
+    assert np.isclose(ef[k3, 1], np.log1p(0.5) / 10) and ef[k3, 2] == 0.0 and ef[k3, 0] == 0.0
     b = make_batch([(node, ei, ef), (node, ei, ef)], "cpu")
     h = b.host
     assert b.n_nodes == 8 and b.n_edges == 2 * ei.shape[1]

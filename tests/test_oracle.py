@@ -177,3 +177,20 @@ def test_cpu_baseline_matches_reference(case):
 def test_z_sample_sums_on_unsigned_bits():
     bits = np.array([[1, 0, 1], [0, 0, 1]], dtype=np.uint8)
     assert list(O.z_sample_sums(bits, ["ZZI", "IIZ", "III"])) == [0, -2, 2]
+
+
+def test_product_workloads_equal_the_oracle_workloads():
+    """bench.py and the benchmarks draw their inputs from vqemps.workloads; the
+    tests from oracle.workloads: the two generators give the same instances."""
+    from oracle import workloads as OW
+    from vqemps import workloads as PW
+    a, b = OW.batched_40q(seed=3, batch=8), PW.batched_40q(seed=3, batch=8)
+    assert a[0]["ops"] == [tuple(o) for o in b[0]["ops"]] and a[1] == b[1]
+    assert np.array_equal(a[2], b[2]) and np.array_equal(a[3], b[3])
+    pa, pb = OW.uneven_partitions(seed=1, partitions=3), PW.uneven_partitions(seed=1, partitions=3)
+    for x, y in zip(pa, pb):
+        assert x[0]["ops"] == y[0]["ops"] and x[1] == y[1] and np.array_equal(x[2], y[2])
+    g1, g2 = OW.gradient_64q(seed=2, batch=2, terms=50), PW.gradient_64q(seed=2, batch=2, terms=50)
+    assert g1[1] == g2[1] and np.array_equal(g1[3], g2[3]) and g1[0]["ops"] == g2[0]["ops"]
+    p1, p2 = OW.plain_12q(1), PW.plain_12q(1)
+    assert p1[1] == p2[1] and np.array_equal(p1[3], p2[3])
