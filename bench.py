@@ -271,8 +271,11 @@ def main():
     flops_step = stats["flops"] * args.batch
     achieved = flops_step / level_s / 1e12
     variant = eng.level_variant(ham, args.batch)
-    kernel = {"simt": "level_kernel (FP64 FMA pipes)", "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
-              "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)"}.get(variant, str(variant))
+    kernel = {"simt": "level_kernel (FP64 FMA pipes)", "simt_pf": "level_pf_kernel (FP64 FMA pipes, cp.async prefetch)",
+              "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
+              "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)",
+              "dmma_pf": "level_mma_pf_kernel (FP64 DMMA tensor cores, cp.async parent prefetch)"}.get(variant,
+                                                                                                    str(variant))
     traffic = profiled_traffic(variant)
     roofline = dict(bound="tensor" if variant and variant.startswith("dmma") else "fp64", achieved=achieved,
                     peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
