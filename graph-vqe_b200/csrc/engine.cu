@@ -20,6 +20,7 @@
 #include "expect_mma.cuh"
 #include "sample.cuh"
 #include "gradient.cuh"
+#include "gradient_mma.cuh"
 
 using namespace vqemps;
 
@@ -162,6 +163,7 @@ struct vqemps_ctx {
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
+  int grad_mma = 1;                     // gradient levels: 1 FP64 DMMA kernels, 0 SIMT kernels
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
@@ -214,6 +216,11 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(level_mma_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelMmaPfSmem));
   grad_set_attributes();
+  cudaFuncSetAttribute(grad_fwd_level_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(GradFwdMmaSmem));
+  cudaFuncSetAttribute(grad_bwd_level_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(GradBwdMmaSmem));
+  if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT")) ctx->grad_mma = std::strcmp(v, "simt") != 0;
   // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the
   // autotuner's timings are meaningless under a serialising profiler.
   if (const char *v = std::getenv("VQEMPS_LEVEL_VARIANT")) {

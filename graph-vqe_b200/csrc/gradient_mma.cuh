@@ -1,0 +1,406 @@
+// Gradient trie levels on the FP64 tensor cores (DMMA, mma.sync m8n8k4 .f64).
+//
+// Same work, outputs and CTA partition as grad_fwd_level_kernel /
+// grad_bwd_level_kernel (gradient.cuh): CTA x of state b owns groups
+// 16x .. 16x + 15 of the level, warp w takes groups w, w + 4, ...; per-CTA
+// partial sums (leaf sums forward, site cotangents backward) are combined by
+// partial_sum_kernel in a fixed order. Complex products are four real DMMA
+// products over 8 x 8 output tiles (expect_mma.cuh gives the fragment layout
+// and the padded shared-memory strides).
+#pragma once
+#include "common.cuh"
+#include "expect.cuh"
+#include "expect_mma.cuh"
+#include "gradient.cuh"
+
+namespace vqemps {
+
+struct GradFwdMmaSmem {
+  cplx A[CHI * MMA_A_STRIDE];
+  cplx R[ENV_ELEMS];
+  cplx E[GLEVEL_WARPS][CHI * MMA_E_STRIDE];
+  cplx S[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];
+  cplx L[GLEVEL_WARPS][ENV_ELEMS];
+};
+
+__device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int b, int g, cplx *E, int lane) {
+  const DevGroup grp = p.groups[g];
+  if (grp.parent_slot < 0) {
+    for (int e = lane; e < ENV_ELEMS; e += 32)
+      E[(e >> 4) * MMA_E_STRIDE + (e & 15)] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
+  } else {
+    const cplx *src = p.env_prev + (size_t)b * p.prev_stride + (size_t)grp.parent_slot * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) cp_async16(E + (e >> 4) * MMA_E_STRIDE + (e & 15), src + e);
+  }
+}
+
+// S panel [S_0 | S_1] = E [A_0 | A_1] (16 x 32, K = 16) into padded S[i][row][col].
+__device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
+  double sr[2][4][2], si[2][4][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) { sr[rt][ct][0] = sr[rt][ct][1] = 0.0; si[rt][ct][0] = si[rt][ct][1] = 0.0; }
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks) {
+    cplx ef[2], pf[4];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * MMA_E_STRIDE + ks * 4 + t];
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) pf[ct] = A[(ks * 4 + t) * MMA_A_STRIDE + ct * 8 + g];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt) {
+      const double er = ef[rt].x, ei = ef[rt].y, nei = -ef[rt].y;
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) {
+        dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
+        dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
+        dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y);
+        dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
+      }
+    }
+  }
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int col = ct * 8 + 2 * t + j;
+        S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(sr[rt][ct][j], si[rt][ct][j]);
+      }
+}
+
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_fwd_level_mma_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GradFwdMmaSmem &sm = *reinterpret_cast<GradFwdMmaSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) sm.A[(e >> 5) * MMA_A_STRIDE + (e & 31)] = ag[e];
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) sm.R[e] = rg[e];
+    for (int e = lane; e < ENV_ELEMS; e += 32) sm.L[warp][e] = cmake(0, 0);
+  }
+  __syncthreads();
+  const cplx *A = sm.A;
+  const cplx *R = sm.R;
+  cplx *E = sm.E[warp];
+  cplx *S = sm.S[warp];
+  cplx *L = sm.L[warp];
+  const int g = lane >> 2, t = lane & 3;
+  const int per_cta = GLEVEL_WARPS * GROUPS_PER_WARP;
+  const int g0 = blockIdx.x * per_cta;
+  const int g1 = min(g0 + per_cta, p.ngroups);
+  int gidx = g0 + warp;
+  if (gidx < g1) {
+    grad_stage_parent(p, b, gidx, E, lane);
+    cp_async_commit();
+  }
+  for (; gidx < g1; gidx += GLEVEL_WARPS) {
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    mma_panel_EA(E, A, S, g, t);
+    __syncwarp();   // E is dead and S complete: prefetch the next parent
+    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
+    cp_async_commit();
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      const int y0 = cls == 0 ? 0 : 1, y1 = cls == 0 ? 1 : 0;
+      double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) ar[rt][ct][j] = ai[rt][ct][j] = br[rt][ct][j] = bi[rt][ct][j] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        cplx a0[2], a1[2], s0[2], s1[2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) {
+          a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
+          a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
+        }
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) {
+          s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+          s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+        }
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
+            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
+            dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
+            dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
+            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
+            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
+            dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
+            dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
+          }
+      }
+      for (int ci = 0; ci < grp.nchild; ++ci) {
+        const DevNode node = p.nodes[grp.child_begin + ci];
+        const bool iz = (node.code == 0 || node.code == 3);
+        if (iz != (cls == 0)) continue;
+        cplx out[2][2][2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const cplx t0 = cmake(ar[rt][ct][j], ai[rt][ct][j]);
+              const cplx t1 = cmake(br[rt][ct][j], bi[rt][ct][j]);
+              if (node.code == 0 || node.code == 1) out[rt][ct][j] = cadd(t0, t1);
+              else if (node.code == 3) out[rt][ct][j] = csub(t0, t1);
+              else { const cplx d = csub(t1, t0); out[rt][ct][j] = cmake(-d.y, d.x); }
+            }
+        if (node.env_slot >= 0) {
+          cplx *dst = p.env_cur + (size_t)b * p.cur_stride + (size_t)node.env_slot * ENV_ELEMS;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+        }
+        if (node.leaf >= 0 && p.leaf_work) {
+          const double cf = p.leaf_coef[node.leaf];
+          double v = 0.0;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) {
+                const int idx = (rt * 8 + g) * CHI + ct * 8 + 2 * t + j;
+                const cplx rv = R[idx];
+                v += out[rt][ct][j].x * rv.x - out[rt][ct][j].y * rv.y;
+                L[idx] = cadd(L[idx], cscale(out[rt][ct][j], cf));
+              }
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) p.leafval[(size_t)b * p.nleaf + node.leaf] = v;
+        }
+      }
+    }
+    __syncwarp();   // S is rewritten by the next parent
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (!p.leaf_work) return;
+  cplx *dst = p.partial + ((size_t)b * gridDim.x + blockIdx.x) * ENV_ELEMS;
+  for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) {
+    cplx acc = sm.L[0][e];
+    for (int w = 1; w < GLEVEL_WARPS; ++w) acc = cadd(acc, sm.L[w][e]);
+    dst[e] = acc;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// backward level on DMMA. Per group (parent E, site A = [A_0 A_1]):
+//   S_i = E A_i;  per Pauli class, D pair from the children's cotangents and
+//   leaf weights (cls 0: D_0 = xa + xb, D_1 = xa - xb with xa, xb of I / Z;
+//   cls 1: D_0 = xa + i xb, D_1 = xa - i xb with xa, xb of X / Y);
+//   Abar_o += 2 S_{src(o)} D_{src(o)},  Y_o += A_{src(o)} D_{src(o)},
+//   src(o) = o (cls 0) or 1 - o (cls 1);  Ebar_parent = sum_i Y_i A_i^H.
+// The site cotangent accumulates in registers over the warp's groups; the
+// warps' panels are combined in a fixed order at the end.
+// ---------------------------------------------------------------------------
+struct GradBwdMmaSmem {
+  cplx A[CHI * MMA_A_STRIDE];
+  cplx R[ENV_ELEMS];
+  cplx E[GLEVEL_WARPS][CHI * MMA_E_STRIDE];
+  cplx S[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];   // S panel, later the Y panel
+  cplx D[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];   // the class's D pair [d][k][c]
+};
+
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_bwd_level_mma_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  GradBwdMmaSmem &sm = *reinterpret_cast<GradBwdMmaSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) sm.A[(e >> 5) * MMA_A_STRIDE + (e & 31)] = ag[e];
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) sm.R[e] = rg[e];
+  }
+  __syncthreads();
+  const cplx *A = sm.A;
+  const cplx *R = sm.R;
+  cplx *E = sm.E[warp];
+  cplx *S = sm.S[warp];
+  cplx *D = sm.D[warp];
+  const int g = lane >> 2, t = lane & 3;
+  // site cotangent panel of this warp: rows rt * 8 + g, cols ct * 8 + 2t + j of [Abar_0 | Abar_1]
+  double abr[2][4][2], abi[2][4][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) { abr[rt][ct][0] = abr[rt][ct][1] = 0.0; abi[rt][ct][0] = abi[rt][ct][1] = 0.0; }
+  const int per_cta = GLEVEL_WARPS * GROUPS_PER_WARP;
+  const int g0 = blockIdx.x * per_cta;
+  const int g1 = min(g0 + per_cta, p.ngroups);
+  int gidx = g0 + warp;
+  if (gidx < g1) {
+    grad_stage_parent(p, b, gidx, E, lane);
+    cp_async_commit();
+  }
+  for (; gidx < g1; gidx += GLEVEL_WARPS) {
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    mma_panel_EA(E, A, S, g, t);
+    __syncwarp();
+    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
+    cp_async_commit();
+    int idx_child[4] = {-1, -1, -1, -1};
+    for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
+    double yr[2][4][2], yi[2][4][2];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) { yr[rt][ct][0] = yr[rt][ct][1] = 0.0; yi[rt][ct][0] = yi[rt][ct][1] = 0.0; }
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      const int ca = idx_child[cls == 0 ? 0 : 1], cbx = idx_child[cls == 0 ? 3 : 2];
+      DevNode na{}, nb{};
+      na.env_slot = nb.env_slot = -1;
+      na.leaf = nb.leaf = -1;
+      if (ca >= 0) na = p.nodes[ca];
+      if (cbx >= 0) nb = p.nodes[cbx];
+      const double cfa = na.leaf >= 0 ? p.leaf_coef[na.leaf] : 0.0;
+      const double cfb = nb.leaf >= 0 ? p.leaf_coef[nb.leaf] : 0.0;
+      const cplx *bara = na.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + na.env_slot) * ENV_ELEMS : nullptr;
+      const cplx *barb = nb.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + nb.env_slot) * ENV_ELEMS : nullptr;
+      __syncwarp();   // the previous class's D is consumed
+      for (int e = lane; e < ENV_ELEMS; e += 32) {
+        const cplx rc = cconj(R[e]);
+        cplx xa = cscale(rc, cfa), xb = cscale(rc, cfb);
+        if (bara) xa = cadd(xa, bara[e]);
+        if (barb) xb = cadd(xb, barb[e]);
+        cplx d0, d1;
+        if (cls == 0) {
+          d0 = cadd(xa, xb);
+          d1 = csub(xa, xb);
+        } else {
+          const cplx ixb = cmake(-xb.y, xb.x);
+          d0 = cadd(xa, ixb);
+          d1 = csub(xa, ixb);
+        }
+        D[(e >> 4) * MMA_S_STRIDE + (e & 15)] = d0;
+        D[(CHI + (e >> 4)) * MMA_S_STRIDE + (e & 15)] = d1;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        // output column tile ct covers panel half o = ct >> 1; operand source src(o)
+        cplx sf[2][2], af[2][2], df[4];
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+          const int src = cls == 0 ? o : 1 - o;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt) {
+            sf[o][rt] = S[(src * CHI + rt * 8 + g) * MMA_S_STRIDE + ks * 4 + t];
+            af[o][rt] = A[(rt * 8 + g) * MMA_A_STRIDE + src * CHI + ks * 4 + t];
+          }
+        }
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) {
+          const int src = cls == 0 ? (ct >> 1) : 1 - (ct >> 1);
+          df[ct] = D[(src * CHI + ks * 4 + t) * MMA_S_STRIDE + (ct & 1) * 8 + g];
+        }
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) {
+            const cplx x = sf[ct >> 1][rt], a = af[ct >> 1][rt], d = df[ct];
+            dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
+            dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
+            dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
+            dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
+            dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
+            dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
+            dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
+            dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
+          }
+      }
+    }
+    if (p.s > 0) {
+      // Y panel into the S region (S is dead), then Ebar_parent = sum_i Y_i A_i^H
+      __syncwarp();
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int col = ct * 8 + 2 * t + j;
+            S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(yr[rt][ct][j], yi[rt][ct][j]);
+          }
+      __syncwarp();
+      double orr[2][2][2], oi[2][2][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) { orr[rt][ct][0] = orr[rt][ct][1] = 0.0; oi[rt][ct][0] = oi[rt][ct][1] = 0.0; }
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks) {
+        const int kk = ks * 4 + t;            // (i, k) = (kk >> 4, kk & 15)
+        cplx yf[2], bf[2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) yf[rt] = S[((kk >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (kk & 15)];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) bf[ct] = A[(ct * 8 + g) * MMA_A_STRIDE + kk];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            // Y conj(A): re = Yr Ar + Yi Ai, im = Yi Ar - Yr Ai
+            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
+            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
+            dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
+            dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
+          }
+      }
+      cplx *dst = p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS;
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = cmake(orr[rt][ct][j], oi[rt][ct][j]);
+    }
+    __syncwarp();   // S / D are rewritten by the next group
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // fixed-order combination of the warps' site cotangent panels (times 2)
+  cplx *panel = sm.S[warp];     // 576 >= 512 entries, one per site element
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int col = ct * 8 + 2 * t + j;
+        panel[((rt * 8 + g) * 2 + (col >> 4)) * CHI + (col & 15)] = cmake(2.0 * abr[rt][ct][j], 2.0 * abi[rt][ct][j]);
+      }
+  __syncthreads();
+  cplx *dst = p.partial + ((size_t)b * gridDim.x + blockIdx.x) * SITE_ELEMS;
+  for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) {
+    cplx acc = sm.S[0][e];
+    for (int w = 1; w < GLEVEL_WARPS; ++w) acc = cadd(acc, sm.S[w][e]);
+    dst[e] = acc;
+  }
+}
+
+}  // namespace vqemps

@@ -262,6 +262,11 @@ class Engine:
         """Keep every `every`-th trie level in the gradient's forward sweep (1: all)."""
         check(self.ctx, self.lib.vqemps_set_grad_checkpoint(self.ctx, int(every)), "set_grad_checkpoint")
 
+    def set_grad_variant(self, variant: str):
+        """Gradient level kernels: 'dmma' (FP64 tensor cores, default) or 'simt'."""
+        check(self.ctx, self.lib.vqemps_set_grad_variant(self.ctx, {"simt": 0, "dmma": 1}[variant]),
+              "set_grad_variant")
+
     def energy_grad(self, ham: Hamiltonian, theta, stream=None):
         """Energies and dE/dtheta through the exact bond-doubling MPS."""
         t = self._theta(theta)

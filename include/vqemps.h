@@ -138,6 +138,10 @@ int vqemps_energy_grad_batch(vqemps_ctx *ctx, int handle, const double *theta_de
  * sweep keeps every `every`-th level, the backward sweep recomputes the rest one
  * segment at a time. Default 8; 1 keeps every level (no recomputation). */
 int vqemps_set_grad_checkpoint(vqemps_ctx *ctx, int every);
+/* Gradient level kernels (no reference counterpart): 1 = FP64 DMMA tensor-core
+ * kernels (default), 0 = SIMT FMA kernels. Both give the same values to rounding;
+ * the environment variable VQEMPS_GRAD_VARIANT=simt selects 0 at creation. */
+int vqemps_set_grad_variant(vqemps_ctx *ctx, int variant);
 
 /* Perfect sampling of B states: shots bitstrings each, bit q of shot s of state
  * b in packed_dev[(b * shots + s) * W + q / 64] >> (q % 64), W = ceil(n / 64),

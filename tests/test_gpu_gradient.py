@@ -29,10 +29,12 @@ def _spec(case):
 @pytest.mark.parametrize("case", [c for c in GOLDEN if c["gradient"] is not None], ids=lambda c: c["name"])
 @pytest.mark.parametrize("order", ["msb", "qubit"])
 @pytest.mark.parametrize("every", [1, 3, 8])
-def test_gradient_matches_reference_golden(vq, case, order, every):
+@pytest.mark.parametrize("variant", ["dmma", "simt"])
+def test_gradient_matches_reference_golden(vq, case, order, every, variant):
     spec = _spec(case)
     eng = vq.Engine(0, 16)
     eng.set_grad_checkpoint(every)
+    eng.set_grad_variant(variant)
     eng.set_spec(spec, site_order=order)
     ham = eng.set_hamiltonian(case["words"], case["coeffs"])
     e, g = eng.energy_grad(ham, np.array(case["x"]))
@@ -91,3 +93,21 @@ def test_checkpointing_is_bitwise_neutral(vq):
         out.append((e.cpu().numpy(), g.cpu().numpy()))
     for e, g in out[1:]:
         assert np.array_equal(e, out[0][0]) and np.array_equal(g, out[0][1])
+
+
+def test_dmma_and_simt_gradient_kernels_agree(vq):
+    """The FP64 tensor-core gradient levels and the SIMT ones compute the same
+    products in another summation order: equal to rounding at 40 qubits."""
+    import torch
+    spec, words, coeffs, thetas = W.batched_40q(seed=4, batch=4, terms=2000)
+    out = {}
+    for variant in ("dmma", "simt"):
+        eng = vq.Engine(0, 16)
+        eng.set_spec(spec)
+        eng.set_grad_variant(variant)
+        ham = eng.set_hamiltonian(words, coeffs)
+        e, g = eng.energy_grad(ham, torch.tensor(thetas, device=eng.device))
+        out[variant] = (e.cpu().numpy(), g.cpu().numpy())
+    (e1, g1), (e2, g2) = out["dmma"], out["simt"]
+    assert np.allclose(e1, e2, rtol=1e-12, atol=1e-9)
+    assert np.abs(g1 - g2).max() <= 1e-10 * max(1.0, np.abs(g2).max())
