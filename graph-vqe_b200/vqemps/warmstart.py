@@ -8,9 +8,10 @@ GPU with the network's own kernels, and the time-to-same-energy comparison.
 The plain method is ``strategy.IndependentPartitionVQE`` (partition warm start,
 local solves, one global L-BFGS-B refinement). The learned method replaces the
 partition warm start by the network's proposal and runs the same global
-refinement from it. Every proposal is judged by the exact MPS energy: if it is
-not finite or not below the energy of the all-zero angles (the |0...0> product
-state, the ansatz's trivial point), the partition warm start runs instead.
+refinement from it. Every proposal is judged by the exact MPS energy, in one
+batched call with the all-zero angles (the |0...0> product state, the ansatz's
+trivial point): the refinement starts from whichever of the two is lower, and
+the partition warm start runs instead when the proposal's energy is not finite.
 """
 from __future__ import annotations
 
@@ -23,6 +24,7 @@ import numpy as np
 import torch
 
 from . import mpnn as M
+from ._lib import EngineError
 from .strategy import GlobalProblem, IndependentPartitionVQE
 from . import workloads as WL
 
@@ -97,8 +99,14 @@ class LearnedWarmStart:
         P = strat.num_params
         theta = self.propose(n, words, coeffs)
         t_prop = time.perf_counter() - t0
-        e_prop, e_zero = (float(v) for v in strat.energy(np.stack([theta, np.zeros(P)])))
-        fallback = not np.isfinite(e_prop) or e_prop >= e_zero
+        try:
+            e_prop, e_zero = (float(v) for v in strat.energy(np.stack([theta, np.zeros(P)])))
+        except EngineError:      # the proposal's state failed (nonfinite angles or SVD)
+            e_prop, e_zero = float("nan"), float(strat.energy(np.zeros((1, P)))[0])
+        fallback = not np.isfinite(e_prop)
+        start = "proposal"
+        if not fallback and e_zero < e_prop:
+            start, theta = "zero", np.zeros(P)
         trace = []
 
         def watch(e):
@@ -108,11 +116,11 @@ class LearnedWarmStart:
 
         reached = None
         try:
-            watch(e_prop)
+            watch(min(e_prop, e_zero) if not fallback else e_prop)
             if fallback:
                 plain, _ = solve_plain(self.engine, n, words, coeffs, global_maxiter=global_maxiter,
                                        energy_tol=energy_tol)
-                return dict(fallback=True, proposal_energy=e_prop, zero_energy=e_zero,
+                return dict(fallback=True, start="partition", proposal_energy=e_prop, zero_energy=e_zero,
                             best_energy=plain["best_energy"], best_params=plain["best_params"], reached_s=None,
                             wall_s=time.perf_counter() - t0)
             base_energy, base_vg = strat.energy, strat.value_grad
@@ -133,7 +141,7 @@ class LearnedWarmStart:
         except _TargetReached:
             reached = trace[-1][0]
             best = trace[-1][1]
-        return dict(fallback=False, proposal_energy=e_prop, zero_energy=e_zero, proposal_s=t_prop,
+        return dict(fallback=False, start=start, proposal_energy=e_prop, zero_energy=e_zero, proposal_s=t_prop,
                     best_energy=min(best, min(e for _, e in trace)), reached_s=reached,
                     wall_s=time.perf_counter() - t0, trace=trace)
 
@@ -232,7 +240,7 @@ def evaluate(params_path, count=20, seed0=900000, n=96, terms=40000, global_maxi
         lw = learned.run(nn, words, coeffs, global_maxiter=global_maxiter, target=target)
         row = dict(seed=seed0 + i, n=nn, terms=len(words), plain_energy=e_plain, plain_s=plain["wall_s"],
                    plain_local_s=plain["local_s"], warm_start_energy=plain["warm_start_energy"],
-                   learned_fallback=lw["fallback"], proposal_energy=lw["proposal_energy"],
+                   learned_fallback=lw["fallback"], learned_start=lw["start"], proposal_energy=lw["proposal_energy"],
                    zero_energy=lw["zero_energy"], learned_best=lw.get("best_energy"),
                    learned_reached_s=lw.get("reached_s"), learned_wall_s=lw["wall_s"])
         row["ratio"] = (row["learned_reached_s"] / row["plain_s"]) if row["learned_reached_s"] else None
@@ -240,6 +248,7 @@ def evaluate(params_path, count=20, seed0=900000, n=96, terms=40000, global_maxi
         print(json.dumps(row), flush=True)
     ok = [r for r in rows if r["ratio"] is not None]
     summary = dict(instances=len(rows), reached=len(ok), fallback=sum(r["learned_fallback"] for r in rows),
+                   started_from_zero=sum(r["learned_start"] == "zero" for r in rows),
                    median_ratio=float(np.median([r["ratio"] for r in ok])) if ok else None,
                    within_half=sum(r["ratio"] <= 0.5 for r in ok))
     print(json.dumps(dict(summary=summary)), flush=True)

@@ -54,14 +54,19 @@ def test_learned_proposal_beats_partition_warm_start(ws):
     assert np.median(ratios) < 1.0
 
 
-def test_bad_proposal_falls_back(ws):
+def test_judgement_and_fallback(ws):
+    """A proposal no better than the all-zero angles starts the refinement from
+    those; a non-finite proposal falls back to the partition warm start."""
     import vqemps
     from vqemps import workloads as WL
     eng = vqemps.Engine(0, 16)
-    zero = np.zeros_like(np.load(WEIGHTS)["params"])          # proposes all-zero angles
-    learned = ws.LearnedWarmStart(eng, zero)
+    shape = np.load(WEIGHTS)["params"].shape
     n, words, coeffs = WL.warm_start_test_problem(5, n=20, terms=400)
-    out = learned.run(n, words, coeffs)
-    assert out["fallback"] and out["proposal_energy"] == out["zero_energy"]
+    zero = ws.LearnedWarmStart(eng, np.zeros(shape, dtype=np.float32))      # proposes all-zero angles
+    out = zero.run(n, words, coeffs)
+    assert not out["fallback"] and out["proposal_energy"] == out["zero_energy"]
+    bad = ws.LearnedWarmStart(eng, np.full(shape, np.nan, dtype=np.float32))
+    out = bad.run(n, words, coeffs)
+    assert out["fallback"] and out["start"] == "partition" and not np.isfinite(out["proposal_energy"])
     plain, _ = ws.solve_plain(eng, n, words, coeffs)
     assert out["best_energy"] == plain["best_energy"]          # the partition warm start ran instead
