@@ -274,7 +274,9 @@ def main():
     kernel = {"simt": "level_kernel (FP64 FMA pipes)", "simt_pf": "level_pf_kernel (FP64 FMA pipes, cp.async prefetch)",
               "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
               "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)",
-              "dmma_pf": "level_mma_pf_kernel (FP64 DMMA tensor cores, cp.async parent prefetch)"}.get(variant,
+              "dmma_pf": "level_mma_pf_kernel (FP64 DMMA tensor cores, cp.async parent prefetch)",
+              "dmma3_pf": "level_mma3_pf_kernel (FP64 DMMA tensor cores, Gauss 3-product complex multiply, "
+                          "cp.async parent prefetch)"}.get(variant,
                                                                                                     str(variant))
     traffic = profiled_traffic(variant)
     roofline = dict(bound="tensor" if variant and variant.startswith("dmma") else "fp64", achieved=achieved,

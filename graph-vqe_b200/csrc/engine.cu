@@ -163,7 +163,7 @@ struct vqemps_ctx {
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
-  int grad_mma = 1;                     // gradient levels: 1 FP64 DMMA kernels, 0 SIMT kernels
+  int grad_mma = 2;                     // gradient levels: 0 SIMT, 1 FP64 DMMA, 2 DMMA with Gauss forward
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
@@ -215,17 +215,22 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
                        (int)sizeof(LevelPfSmem));
   cudaFuncSetAttribute(level_mma_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelMmaPfSmem));
+  cudaFuncSetAttribute(level_mma3_pf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(LevelMmaPfSmem));
   grad_set_attributes();
   cudaFuncSetAttribute(grad_fwd_level_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradFwdMmaSmem));
   cudaFuncSetAttribute(grad_bwd_level_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradBwdMmaSmem));
-  if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT")) ctx->grad_mma = std::strcmp(v, "simt") != 0;
+  cudaFuncSetAttribute(grad_fwd_level_mma3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(GradFwdMmaSmem));
+  if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT"))
+    ctx->grad_mma = std::strcmp(v, "simt") == 0 ? 0 : std::strcmp(v, "dmma") == 0 ? 1 : 2;
   // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the
   // autotuner's timings are meaningless under a serialising profiler.
   if (const char *v = std::getenv("VQEMPS_LEVEL_VARIANT")) {
-    static const char *names[] = {"simt", "dmma4", "dmma8", "simt_pf", "dmma_pf"};
-    for (int i = 0; i < 5; ++i)
+    static const char *names[] = {"simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf"};
+    for (int i = 0; i < 6; ++i)
       if (std::strcmp(v, names[i]) == 0 || (v[0] == '0' + i && v[1] == 0)) ctx->forced_variant = i;
   }
   *out = ctx;
@@ -707,7 +712,7 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
 }
 
 // Level kernel variants: the autotuner times each on the caller's workload.
-enum : int { LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_COUNT = 5 };
+enum : int { LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5, LV_COUNT = 6 };
 
 static void launch_level_variant(int variant, const LevelParams &lp, int ng, int B, cudaStream_t st) {
   switch (variant) {
@@ -728,6 +733,12 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
       const int gpw = ng >= 4 * MPF_WARPS ? 4 : 1;
       const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
       level_mma_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
+      break;
+    }
+    case LV_MMA3PF4: {
+      const int gpw = ng >= 4 * MPF_WARPS ? 4 : 1;
+      const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
+      level_mma3_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
     }
     default:

@@ -217,9 +217,14 @@ __device__ __forceinline__ void stage_parent_padded(const LevelParams &p, int b,
   }
 }
 
-__global__ void __launch_bounds__(MPF_WARPS * 32, 3)
-level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// GAUSS selects the complex product: false = four real DMMA products
+// (Re = XrYr - XiYi, Im = XrYi + XiYr); true = Gauss's three-product form
+// k1 = Yr (Xr + Xi), k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi), Re = k1 - k3,
+// Im = k1 + k2, which trades a quarter of the tensor-pipe work for operand sums
+// on the FMA pipe and a third accumulator.
+template <bool GAUSS>
+__device__ __forceinline__ void level_mma_pf_body(const LevelParams &p, int groups_per_warp,
+                                                  unsigned char *smem_raw) {
   LevelMmaPfSmem &sm = *reinterpret_cast<LevelMmaPfSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // uniform batch: state blockIdx.y, groups interleaved over the grid;
@@ -257,7 +262,7 @@ level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    {
+    if constexpr (!GAUSS) {
       double sr[2][4][2], si[2][4][2];
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
@@ -291,6 +296,43 @@ level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
             const int col = ct * 8 + 2 * t + j;
             S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(sr[rt][ct][j], si[rt][ct][j]);
           }
+    } else {
+      // S = E A with X = E (row operand), Y = A (column operand)
+      double k1[2][4][2], k2[2][4][2], k3[2][4][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) k1[rt][ct][j] = k2[rt][ct][j] = k3[rt][ct][j] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        cplx ef[2], pf[4];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * MMA_E_STRIDE + ks * 4 + t];
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) pf[ct] = A[(ks * 4 + t) * MMA_A_STRIDE + ct * 8 + g];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) {
+          const double xs = ef[rt].x + ef[rt].y;
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) {
+            dmma(k1[rt][ct][0], k1[rt][ct][1], xs, pf[ct].x);
+            dmma(k2[rt][ct][0], k2[rt][ct][1], ef[rt].x, pf[ct].y - pf[ct].x);
+            dmma(k3[rt][ct][0], k3[rt][ct][1], ef[rt].y, pf[ct].x + pf[ct].y);
+          }
+        }
+      }
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int col = ct * 8 + 2 * t + j;
+            S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] =
+                cmake(k1[rt][ct][j] - k3[rt][ct][j], k1[rt][ct][j] + k2[rt][ct][j]);
+          }
     }
     __syncwarp();   // E is dead and S is complete: prefetch the next parent
     if (k + 1 < count) stage_parent_padded(p, b, gidx + stride, E, lane);
@@ -305,32 +347,84 @@ level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
         for (int ct = 0; ct < 2; ++ct)
 #pragma unroll
           for (int j = 0; j < 2; ++j) ar[rt][ct][j] = ai[rt][ct][j] = br[rt][ct][j] = bi[rt][ct][j] = 0.0;
+      if constexpr (!GAUSS) {
 #pragma unroll
-      for (int ks = 0; ks < 4; ++ks) {
-        cplx a0[2], a1[2], s0[2], s1[2];
+        for (int ks = 0; ks < 4; ++ks) {
+          cplx a0[2], a1[2], s0[2], s1[2];
 #pragma unroll
-        for (int rt = 0; rt < 2; ++rt) {
-          a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
-          a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
+          for (int rt = 0; rt < 2; ++rt) {
+            a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
+            a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
+          }
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+            s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+          }
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = 0; ct < 2; ++ct) {
+              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
+              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
+              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
+              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
+            }
         }
+      } else {
+        // conj(X) Y with X = A_i, Y = S: k1 = Yr (Xr - Xi), k2 = Xr (Yi - Yr),
+        // k3 = -Xi (Yr + Yi); k1 and k3 accumulate in ar / br (then ar = k1 - k3),
+        // k2 in ai / bi (then ai = k1 + k2)
+        double a3[2][2][2], b3[2][2][2];
 #pragma unroll
-        for (int ct = 0; ct < 2; ++ct) {
-          s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-          s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) a3[rt][ct][j] = b3[rt][ct][j] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks) {
+          cplx a0[2], a1[2], s0[2], s1[2];
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt) {
+            a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
+            a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
+          }
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+            s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+          }
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt) {
+            const double xd0 = a0[rt].x - a0[rt].y, xd1 = a1[rt].x - a1[rt].y;
+#pragma unroll
+            for (int ct = 0; ct < 2; ++ct) {
+              dmma(ar[rt][ct][0], ar[rt][ct][1], xd0, s0[ct].x);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y - s0[ct].x);
+              dmma(a3[rt][ct][0], a3[rt][ct][1], -a0[rt].y, s0[ct].x + s0[ct].y);
+              dmma(br[rt][ct][0], br[rt][ct][1], xd1, s1[ct].x);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y - s1[ct].x);
+              dmma(b3[rt][ct][0], b3[rt][ct][1], -a1[rt].y, s1[ct].x + s1[ct].y);
+            }
+          }
         }
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-          for (int ct = 0; ct < 2; ++ct) {
-            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
-            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
-            dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
-            dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
-            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
-            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
-            dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
-            dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
-          }
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const double k1a = ar[rt][ct][j], k1b = br[rt][ct][j];
+              ar[rt][ct][j] = k1a - a3[rt][ct][j];
+              ai[rt][ct][j] = k1a + ai[rt][ct][j];
+              br[rt][ct][j] = k1b - b3[rt][ct][j];
+              bi[rt][ct][j] = k1b + bi[rt][ct][j];
+            }
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
         const DevNode node = p.nodes[grp.child_begin + ci];
@@ -377,6 +471,20 @@ level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
     __syncwarp();   // S is rewritten by the next parent
   }
   cp_async_wait<0>();
+}
+
+__global__ void __launch_bounds__(MPF_WARPS * 32, 3)
+level_mma_pf_kernel(LevelParams p, int groups_per_warp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  level_mma_pf_body<false>(p, groups_per_warp, smem_raw);
+}
+
+// The same level with Gauss's three-product complex multiply (a quarter fewer
+// DMMA issues per product).
+__global__ void __launch_bounds__(MPF_WARPS * 32, 3)
+level_mma3_pf_kernel(LevelParams p, int groups_per_warp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  level_mma_pf_body<true>(p, groups_per_warp, smem_raw);
 }
 
 }  // namespace vqemps

@@ -34,13 +34,22 @@ __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int 
   }
 }
 
-// S panel [S_0 | S_1] = E [A_0 | A_1] (16 x 32, K = 16) into padded S[i][row][col].
+// S panel [S_0 | S_1] = E [A_0 | A_1] (16 x 32, K = 16) into padded S[i][row][col];
+// GAUSS: three real products per complex product (k1 = Yr (Xr + Xi),
+// k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2).
+template <bool GAUSS = false>
 __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
-  double sr[2][4][2], si[2][4][2];
+  double sr[2][4][2], si[2][4][2], s3[GAUSS ? 2 : 1][4][2];
 #pragma unroll
   for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
     for (int ct = 0; ct < 4; ++ct) { sr[rt][ct][0] = sr[rt][ct][1] = 0.0; si[rt][ct][0] = si[rt][ct][1] = 0.0; }
+  if constexpr (GAUSS) {
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) s3[rt][ct][0] = s3[rt][ct][1] = 0.0;
+  }
 #pragma unroll
   for (int ks = 0; ks < 4; ++ks) {
     cplx ef[2], pf[4];
@@ -53,10 +62,16 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
       const double er = ef[rt].x, ei = ef[rt].y, nei = -ef[rt].y;
 #pragma unroll
       for (int ct = 0; ct < 4; ++ct) {
-        dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
-        dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
-        dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y);
-        dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
+        if constexpr (GAUSS) {
+          dmma(sr[rt][ct][0], sr[rt][ct][1], er + ei, pf[ct].x);                 // k1
+          dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y - pf[ct].x);           // k2
+          dmma(s3[rt][ct][0], s3[rt][ct][1], ei, pf[ct].x + pf[ct].y);           // k3
+        } else {
+          dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
+          dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
+          dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y);
+          dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
+        }
       }
     }
   }
@@ -67,13 +82,15 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int col = ct * 8 + 2 * t + j;
-        S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(sr[rt][ct][j], si[rt][ct][j]);
+        cplx v;
+        if constexpr (GAUSS) v = cmake(sr[rt][ct][j] - s3[rt][ct][j], sr[rt][ct][j] + si[rt][ct][j]);
+        else v = cmake(sr[rt][ct][j], si[rt][ct][j]);
+        S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = v;
       }
 }
 
-__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
-grad_fwd_level_mma_kernel(GradLevelParams p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+template <bool GAUSS>
+__device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradFwdMmaSmem &sm = *reinterpret_cast<GradFwdMmaSmem *>(smem_raw);
   const int b = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -103,7 +120,7 @@ grad_fwd_level_mma_kernel(GradLevelParams p) {
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    mma_panel_EA(E, A, S, g, t);
+    mma_panel_EA<GAUSS>(E, A, S, g, t);
     __syncwarp();   // E is dead and S complete: prefetch the next parent
     if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
     cp_async_commit();
@@ -117,6 +134,15 @@ grad_fwd_level_mma_kernel(GradLevelParams p) {
         for (int ct = 0; ct < 2; ++ct)
 #pragma unroll
           for (int j = 0; j < 2; ++j) ar[rt][ct][j] = ai[rt][ct][j] = br[rt][ct][j] = bi[rt][ct][j] = 0.0;
+      double a3[GAUSS ? 2 : 1][2][2], b3[GAUSS ? 2 : 1][2][2];
+      if constexpr (GAUSS) {
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) a3[rt][ct][j] = b3[rt][ct][j] = 0.0;
+      }
 #pragma unroll
       for (int ks = 0; ks < 4; ++ks) {
         cplx a0[2], a1[2], s0[2], s1[2];
@@ -134,15 +160,39 @@ grad_fwd_level_mma_kernel(GradLevelParams p) {
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
           for (int ct = 0; ct < 2; ++ct) {
-            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
-            dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
-            dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
-            dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
-            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
-            dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
-            dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
-            dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
+            if constexpr (GAUSS) {
+              // conj(X) Y: k1 = Yr (Xr - Xi) -> ar, k2 = Xr (Yi - Yr) -> ai, k3 = -Xi (Yr + Yi) -> a3
+              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x - a0[rt].y, s0[ct].x);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y - s0[ct].x);
+              dmma(a3[rt][ct][0], a3[rt][ct][1], -a0[rt].y, s0[ct].x + s0[ct].y);
+              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x - a1[rt].y, s1[ct].x);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y - s1[ct].x);
+              dmma(b3[rt][ct][0], b3[rt][ct][1], -a1[rt].y, s1[ct].x + s1[ct].y);
+            } else {
+              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
+              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
+              dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
+              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
+              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
+              dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
+            }
           }
+      }
+      if constexpr (GAUSS) {
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const double k1a = ar[rt][ct][j], k1b = br[rt][ct][j];
+              ar[rt][ct][j] = k1a - a3[rt][ct][j];
+              ai[rt][ct][j] = k1a + ai[rt][ct][j];
+              br[rt][ct][j] = k1b - b3[rt][ct][j];
+              bi[rt][ct][j] = k1b + bi[rt][ct][j];
+            }
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
         const DevNode node = p.nodes[grp.child_begin + ci];
@@ -200,6 +250,19 @@ grad_fwd_level_mma_kernel(GradLevelParams p) {
     for (int w = 1; w < GLEVEL_WARPS; ++w) acc = cadd(acc, sm.L[w][e]);
     dst[e] = acc;
   }
+}
+
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_fwd_level_mma_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_fwd_level_mma_body<false>(p, smem_raw);
+}
+
+// Forward gradient level with Gauss's three-product complex multiply.
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_fwd_level_mma3_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_fwd_level_mma_body<true>(p, smem_raw);
 }
 
 // ---------------------------------------------------------------------------

@@ -201,10 +201,10 @@ class Engine:
     def free_hamiltonian(self, ham: Hamiltonian):
         check(self.ctx, self.lib.vqemps_free_hamiltonian(self.ctx, ham.handle), "free_hamiltonian")
 
-    LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf")
+    LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf")
 
     def set_level_variant(self, variant):
-        """Force a trie-level kernel ('simt', 'dmma4', 'dmma8', 'simt_pf', 'dmma_pf') or None to autotune."""
+        """Force a trie-level kernel (one of LEVEL_VARIANTS) or None to autotune."""
         v = -1 if variant is None else self.LEVEL_VARIANTS.index(variant)
         check(self.ctx, self.lib.vqemps_set_level_variant(self.ctx, v), "set_level_variant")
 
@@ -263,8 +263,8 @@ class Engine:
         check(self.ctx, self.lib.vqemps_set_grad_checkpoint(self.ctx, int(every)), "set_grad_checkpoint")
 
     def set_grad_variant(self, variant: str):
-        """Gradient level kernels: 'dmma' (FP64 tensor cores, default) or 'simt'."""
-        check(self.ctx, self.lib.vqemps_set_grad_variant(self.ctx, {"simt": 0, "dmma": 1}[variant]),
+        """Gradient level kernels: 'dmma3' (FP64 tensor cores, Gauss forward; default), 'dmma' or 'simt'."""
+        check(self.ctx, self.lib.vqemps_set_grad_variant(self.ctx, {"simt": 0, "dmma": 1, "dmma3": 2}[variant]),
               "set_grad_variant")
 
     def energy_grad(self, ham: Hamiltonian, theta, stream=None):

@@ -138,9 +138,10 @@ int vqemps_energy_grad_batch(vqemps_ctx *ctx, int handle, const double *theta_de
  * sweep keeps every `every`-th level, the backward sweep recomputes the rest one
  * segment at a time. Default 8; 1 keeps every level (no recomputation). */
 int vqemps_set_grad_checkpoint(vqemps_ctx *ctx, int every);
-/* Gradient level kernels (no reference counterpart): 1 = FP64 DMMA tensor-core
- * kernels (default), 0 = SIMT FMA kernels. Both give the same values to rounding;
- * the environment variable VQEMPS_GRAD_VARIANT=simt selects 0 at creation. */
+/* Gradient level kernels (no reference counterpart): 0 = SIMT FMA kernels,
+ * 1 = FP64 DMMA tensor-core kernels, 2 = DMMA with Gauss's three-product complex
+ * multiply in the forward levels (default). All give the same values to
+ * rounding; VQEMPS_GRAD_VARIANT (simt, dmma, dmma3) selects one at creation. */
 int vqemps_set_grad_variant(vqemps_ctx *ctx, int variant);
 
 /* Perfect sampling of B states: shots bitstrings each, bit q of shot s of state
@@ -170,17 +171,18 @@ int vqemps_sampled_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, 
                           uint64_t seed, int rng, int mode, double *energies_dev,
                           double *per_term_dev, void *stream);
 
-/* Level-kernel selection (no reference counterpart). The trie levels have five
+/* Level-kernel selection (no reference counterpart). The trie levels have six
  * implementations: 0 FP64 CUDA-core (SIMT) kernel, 1 FP64 tensor-core (DMMA)
  * kernel with 4 warps per CTA, 2 DMMA with 8 warps per CTA, 3 SIMT with
  * persistent warps that prefetch the next parent environment (cp.async),
- * 4 DMMA with the same prefetching pipeline. By default the
+ * 4 DMMA with the same prefetching pipeline, 5 the same with Gauss's
+ * three-product complex multiply. By default the
  * engine times each once per plan and batch-size bucket (powers of two) on the
  * first call and keeps the fastest (that first call synchronises its stream);
  * vqemps_set_level_variant forces one (-1 restores tuning);
  * vqemps_level_variant reports the one in use (-1: not tuned yet). The
  * environment variable VQEMPS_LEVEL_VARIANT (simt, dmma4, dmma8, simt_pf,
- * dmma_pf or 0-4), read by vqemps_create, forces one for every context. */
+ * dmma_pf, dmma3_pf or 0-5), read by vqemps_create, forces one for every context. */
 int vqemps_set_level_variant(vqemps_ctx *ctx, int variant);
 int vqemps_level_variant(vqemps_ctx *ctx, int handle, int B, int *variant);
 

@@ -36,7 +36,7 @@ def _engine(vq, spec, max_bond=16, order="msb"):
     return eng
 
 
-@pytest.mark.parametrize("variant", ["simt", "dmma4", "dmma8", "simt_pf", "dmma_pf"])
+@pytest.mark.parametrize("variant", ["simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf"])
 @pytest.mark.parametrize("order", ["msb", "qubit"])
 @pytest.mark.parametrize("case", GOLDEN, ids=[c["name"] for c in GOLDEN])
 def test_energy_matches_reference_golden(vq, case, order, variant):
@@ -121,7 +121,7 @@ def test_two_qubit_closed_form_and_widths(vq):
         assert abs(float(eng.energy(ham, [t])[0]) - (math.cos(t) + 0.25)) < 1e-10
 
 
-@pytest.mark.parametrize("variant", ["simt", "dmma4"])
+@pytest.mark.parametrize("variant", ["simt", "dmma4", "dmma3_pf"])
 def test_batch_equals_single_calls_bitwise(vq, variant):
     spec, words, coeffs, theta = W.plain_12q(0)
     eng = _engine(vq, spec)
@@ -184,7 +184,7 @@ def test_gates_constant_and_custom_matrices(vq):
         assert abs(float(eng.energy(ham, x)[0]) - ref) < 1e-11
 
 
-@pytest.mark.parametrize("variant", [None, "simt", "dmma4", "dmma8", "simt_pf", "dmma_pf"])
+@pytest.mark.parametrize("variant", [None, "simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf"])
 def test_config_40q_batch_energy_parity_sample(vq, variant):
     """40 qubits, 5,000 terms: a few probes of the SPSA batch against the oracle,
     with every trie-level kernel variant and with the autotuner's choice."""
@@ -193,7 +193,7 @@ def test_config_40q_batch_energy_parity_sample(vq, variant):
     eng.set_level_variant(variant)
     ham = eng.set_hamiltonian(words, coeffs)
     e = eng.energy(ham, thetas).cpu().numpy()
-    assert eng.level_variant(ham, 16) in ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf")
+    assert eng.level_variant(ham, 16) in vq.Engine.LEVEL_VARIANTS
     for b in (0, 9):
         ref = float(np.dot(O.expect_words(O.svd_evolve(spec, thetas[b], 16), words).real, coeffs))
         assert abs(e[b] - ref) <= RTOL * max(1.0, abs(ref))

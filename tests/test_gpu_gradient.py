@@ -29,7 +29,7 @@ def _spec(case):
 @pytest.mark.parametrize("case", [c for c in GOLDEN if c["gradient"] is not None], ids=lambda c: c["name"])
 @pytest.mark.parametrize("order", ["msb", "qubit"])
 @pytest.mark.parametrize("every", [1, 3, 8])
-@pytest.mark.parametrize("variant", ["dmma", "simt"])
+@pytest.mark.parametrize("variant", ["dmma3", "dmma", "simt"])
 def test_gradient_matches_reference_golden(vq, case, order, every, variant):
     spec = _spec(case)
     eng = vq.Engine(0, 16)
@@ -101,13 +101,15 @@ def test_dmma_and_simt_gradient_kernels_agree(vq):
     import torch
     spec, words, coeffs, thetas = W.batched_40q(seed=4, batch=4, terms=2000)
     out = {}
-    for variant in ("dmma", "simt"):
+    for variant in ("dmma3", "dmma", "simt"):
         eng = vq.Engine(0, 16)
         eng.set_spec(spec)
         eng.set_grad_variant(variant)
         ham = eng.set_hamiltonian(words, coeffs)
         e, g = eng.energy_grad(ham, torch.tensor(thetas, device=eng.device))
         out[variant] = (e.cpu().numpy(), g.cpu().numpy())
-    (e1, g1), (e2, g2) = out["dmma"], out["simt"]
-    assert np.allclose(e1, e2, rtol=1e-12, atol=1e-9)
-    assert np.abs(g1 - g2).max() <= 1e-10 * max(1.0, np.abs(g2).max())
+    e2, g2 = out["simt"]
+    for variant in ("dmma3", "dmma"):
+        e1, g1 = out[variant]
+        assert np.allclose(e1, e2, rtol=1e-12, atol=1e-9)
+        assert np.abs(g1 - g2).max() <= 1e-10 * max(1.0, np.abs(g2).max())

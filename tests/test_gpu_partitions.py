@@ -45,7 +45,7 @@ def _load(vq, eng, parts, order="msb"):
 def _single(vq, spec, words, coeffs, order="msb"):
     eng = vq.Engine(0, 16)
     eng.set_spec(spec, site_order=order)
-    eng.set_level_variant("dmma_pf")
+    eng.set_level_variant("dmma3_pf")
     return eng, eng.set_hamiltonian(words, coeffs)
 
 
