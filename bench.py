@@ -159,13 +159,18 @@ def measure_fp64_peak(torch, device):
     return best
 
 
+PROFILED = {"dmma_pf": "level_mma_pf_kernel_40q.md", "dmma3_pf": "level_mma3_pf_kernel_40q.md"}
+
+
 def profiled_traffic(variant):
     """DRAM bytes per evaluation of all trie levels, from the committed ncu summary
-    of the same kernel (profiles/level_mma_pf_kernel_40q.md: sum of
-    dram__bytes_read.sum + dram__bytes_write.sum over the 40 level launches of one
-    step at B = 32, divided by 32); None for kernels without such a capture."""
-    path = ROOT / "profiles" / "level_mma_pf_kernel_40q.md"
-    if variant != "dmma_pf" or not path.exists():
+    of the same kernel (profiles/<kernel>_40q.md: sum of dram__bytes_read.sum +
+    dram__bytes_write.sum over the 40 level launches of one step at B = 32,
+    divided by 32); None for kernels without such a capture."""
+    if variant not in PROFILED:
+        return None
+    path = ROOT / "profiles" / PROFILED[variant]
+    if not path.exists():
         return None
     import re
     m = re.search(r"traffic_bytes_per_eval:\s*([0-9.eE+]+)", path.read_text())
