@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <array>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -62,11 +63,41 @@ struct Hamiltonian {
   int32_t *d_sumidx_shared = nullptr;    // T: t for I/Z words, -1 for X/Y words
   int32_t *d_sumidx_word = nullptr;      // T: list position, -2 identity, -1 X/Y
   int32_t *d_wordlist = nullptr;         // nzwords word ids then nzwords last sites
+  // Split evaluation at a cut site c (cut < 0: the prefix trie alone). Terms
+  // ending before c close in the prefix trie's levels 0..c-1; the others pair a
+  // prefix environment after site c-1 with a suffix environment of sites c..n-1
+  // from a suffix trie (one 16 x 16 dot product per distinct pair).
+  int cut = -1;
+  std::vector<int32_t> term_slot;        // T x n: env slot of term t's prefix node at level s (-1 none)
+  std::vector<double> level_flops;       // prefix trie flops per level
+  std::vector<DevGroup> sl_groups;       // prefix levels 0..cut-1 with split leaf ids
+  std::vector<DevNode> sl_nodes;
+  std::vector<int> sr_group_off, sr_node_off, sr_nslot;   // suffix levels, indexed by site (n + 1 / n)
+  std::vector<DevGroup> sr_groups;
+  std::vector<DevNode> sr_nodes;
+  std::vector<int32_t> pairs;            // (prefix slot, suffix slot, leaf) per pair, by prefix slot
+  std::vector<double> split_leaf_coef;
+  std::vector<int32_t> split_term_leaf;
+  int split_nleaf = 0, split_identity_leaf = -1, npairs = 0;
+  int sl_max_slot = 1, sr_max_slot = 1;
+  double split_flops = 0.0;
+  long long split_node_sites = 0;
+  DevGroup *d_sl_groups = nullptr, *d_sr_groups = nullptr;
+  DevNode *d_sl_nodes = nullptr, *d_sr_nodes = nullptr;
+  int32_t *d_pairs = nullptr, *d_split_term_leaf = nullptr;
+  double *d_split_leaf_coef = nullptr;
   ~Hamiltonian() {
     cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_leaf_coef); cudaFree(d_term_leaf);
     cudaFree(d_zmask); cudaFree(d_offdiag); cudaFree(d_codes); cudaFree(d_coeffs);
     cudaFree(d_sumidx_shared); cudaFree(d_sumidx_word); cudaFree(d_wordlist);
+    cudaFree(d_sl_groups); cudaFree(d_sr_groups); cudaFree(d_sl_nodes); cudaFree(d_sr_nodes);
+    cudaFree(d_pairs); cudaFree(d_split_term_leaf); cudaFree(d_split_leaf_coef);
   }
+  // leaves of the energy path (split plan when cut >= 0)
+  int e_nleaf() const { return cut >= 0 ? split_nleaf : nleaf; }
+  int e_identity_leaf() const { return cut >= 0 ? split_identity_leaf : identity_leaf; }
+  const double *e_leaf_coef() const { return cut >= 0 ? d_split_leaf_coef : d_leaf_coef; }
+  const int32_t *e_term_leaf() const { return cut >= 0 ? d_split_term_leaf : d_term_leaf; }
 };
 
 // A partition set: K independent circuits with their own widths, parameters
@@ -151,7 +182,7 @@ struct vqemps_ctx {
   std::map<int, std::unique_ptr<PartSet>> parts;
   int next_handle = 1;
   // workspaces
-  DevBuf<cplx> sites, right, env0, env1;
+  DevBuf<cplx> sites, right, env0, env1, env2, env3, sites_t;
   DevBuf<int32_t> bonds_ws, status;
   DevBuf<double> leafval, theta_stage, energy_stage, per_term_stage;
   DevBuf<uint64_t> bits, seeds;
@@ -164,6 +195,7 @@ struct vqemps_ctx {
   int forced_variant = -1;              // level kernel variant, -1: autotune
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
   int grad_mma = 2;                     // gradient levels: 0 SIMT, 1 FP64 DMMA, 2 DMMA with Gauss forward
+  int split_mode = -1;                  // split evaluation: -1 when it saves work, 0 never, 1 always
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
@@ -243,6 +275,7 @@ extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
   ctx->hams.clear();
   ctx->parts.clear();
   ctx->sites.release(); ctx->right.release(); ctx->env0.release(); ctx->env1.release();
+  ctx->env2.release(); ctx->env3.release(); ctx->sites_t.release();
   ctx->bonds_ws.release(); ctx->status.release(); ctx->leafval.release();
   ctx->theta_stage.release(); ctx->energy_stage.release(); ctx->per_term_stage.release();
   ctx->bits.release(); ctx->zsum.release(); ctx->seeds.release(); ctx->branch.release();
@@ -454,6 +487,8 @@ extern "C" int vqemps_bond_dims(const vqemps_ctx *ctx, int *dims) {
   return VQEMPS_OK;
 }
 
+#include "split_plan.inc"
+
 // ---------------------------------------------------------------------------
 // Hamiltonian plan: one prefix trie over the sorted site-order words, each path
 // cut after its term's last non-identity site.
@@ -534,6 +569,8 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   h->group_off.assign(n + 1, 0);
   h->node_off.assign(n + 1, 0);
   h->nslot.assign(n, 0);
+  h->term_slot.assign((size_t)T * n, -1);
+  h->level_flops.assign(n, 0.0);
   const std::vector<int> &bd = ctx->bonds;
   for (int s = 0; s < n; ++s) {
     h->group_off[s] = (int)h->groups.size();
@@ -581,6 +618,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         h->nodes[h->node_off[s] + k].env_slot = slot_of[k];
       }
     h->nslot[s] = slots;
+    for (size_t j = 0; j < active.size(); ++j) h->term_slot[(size_t)active[j] * n + s] = slot_of[node_of[j]];
     h->max_slot = std::max(h->max_slot, slots);
     // groups: consecutive nodes with the same parent
     {
@@ -602,9 +640,11 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         h->groups.push_back(g);
         // flop accounting with the actual bond dims (dl x dr site)
         const double dl = bd[s], dr = bd[s + 1];
-        h->flops += 8.0 * 2.0 * dl * dl * dr;                               // S_i = E A_i
-        h->flops += ((g.classes & 1) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr;  // I/Z products
-        h->flops += ((g.classes & 2) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr;  // X/Y products
+        const double gf = 8.0 * 2.0 * dl * dl * dr                          // S_i = E A_i
+                          + ((g.classes & 1) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr  // I/Z products
+                          + ((g.classes & 2) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr; // X/Y products
+        h->flops += gf;
+        h->level_flops[s] += gf;
         h->flops_survey += (lastn - first + 1) * 16.0 * dl * dr * (dl + dr);
         h->node_sites += lastn - first + 1;
       }
@@ -615,6 +655,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   }
   h->group_off[n] = (int)h->groups.size();
   h->node_off[n] = (int)h->nodes.size();
+  build_split_plan(*h, code, last, ctx->bonds, ctx->split_mode);
   // upload
   auto up = [&](auto *&dst, const auto &vec) -> cudaError_t {
     using E = typename std::remove_reference<decltype(vec)>::type::value_type;
@@ -635,6 +676,15 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   CUDA_TRY(ctx, up(h->d_sumidx_shared, sumidx_shared));
   CUDA_TRY(ctx, up(h->d_sumidx_word, sumidx_word));
   CUDA_TRY(ctx, up(h->d_wordlist, wl));
+  if (h->cut >= 0) {
+    CUDA_TRY(ctx, up(h->d_sl_groups, h->sl_groups));
+    CUDA_TRY(ctx, up(h->d_sl_nodes, h->sl_nodes));
+    CUDA_TRY(ctx, up(h->d_sr_groups, h->sr_groups));
+    CUDA_TRY(ctx, up(h->d_sr_nodes, h->sr_nodes));
+    CUDA_TRY(ctx, up(h->d_pairs, h->pairs));
+    CUDA_TRY(ctx, up(h->d_split_leaf_coef, h->split_leaf_coef));
+    CUDA_TRY(ctx, up(h->d_split_term_leaf, h->split_term_leaf));
+  }
   const int id = ctx->next_handle++;
   ctx->hams[id] = std::move(h);
   *handle = id;
@@ -656,12 +706,17 @@ extern "C" int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stat
   auto it = ctx->hams.find(handle);
   if (it == ctx->hams.end()) return VQEMPS_INVALID;
   const Hamiltonian &h = *it->second;
-  stats[0] = h.flops;
+  const bool split = h.cut >= 0;
+  stats[0] = split ? h.split_flops : h.flops;
   stats[1] = h.flops_survey;
-  stats[2] = (double)h.node_sites;
-  stats[3] = (double)h.groups.size();
-  stats[4] = (double)h.nleaf;
-  stats[5] = (double)h.max_slot;
+  stats[2] = split ? (double)h.split_node_sites : (double)h.node_sites;
+  stats[3] = split ? (double)(h.sl_groups.size() + h.sr_groups.size()) : (double)h.groups.size();
+  stats[4] = (double)h.e_nleaf();
+  stats[5] = split ? (double)std::max(h.sl_max_slot, h.sr_max_slot) : (double)h.max_slot;
+  stats[6] = (double)h.cut;
+  stats[7] = h.flops;
+  stats[8] = (double)h.node_sites;
+  stats[9] = (double)h.npairs;
   return VQEMPS_OK;
 }
 
@@ -702,11 +757,11 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
 // Identity right environments (and the sampler's branch matrices when branch
 // is non-null); writes the norm into the identity leaf of h when given.
 static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st, cplx *branch) {
-  const int nleaf = h ? std::max(h->nleaf, 1) : 0;
+  const int nleaf = h ? std::max(h->e_nleaf(), 1) : 0;
   if (h) CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
   right_env_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
                                                ctx->status.ptr, h ? ctx->leafval.ptr : nullptr,
-                                               nleaf, h ? h->identity_leaf : -1);
+                                               nleaf, h ? h->e_identity_leaf() : -1);
   CUDA_TRY(ctx, cudaGetLastError());
   return VQEMPS_OK;
 }
@@ -749,9 +804,38 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
 // All trie levels of one evaluation with a given variant (needs launch_right first).
 static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int variant) {
   const int n = ctx->n;
-  const int nleaf = std::max(h.nleaf, 1);
+  const int nleaf = std::max(h.e_nleaf(), 1);
+  const bool split = h.cut >= 0;
+  const int top = split ? h.cut : n;                // prefix levels run on sites 0 .. top - 1
+  if (split) {
+    // suffix levels n-1 .. cut on transposed site tensors, starting from R_{l+1}
+    transpose_sites_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    cplx *renv[2] = {ctx->env2.ptr, ctx->env3.ptr};
+    for (int s = n - 1; s >= h.cut; --s) {
+      const int ng = h.sr_group_off[s + 1] - h.sr_group_off[s];
+      if (ng == 0) continue;                        // sites beyond every term's last
+      LevelParams lp{};
+      lp.sites = ctx->sites_t.ptr;
+      lp.right = ctx->right.ptr;
+      lp.env_prev = renv[(s + 1) & 1];
+      lp.env_cur = renv[s & 1];
+      lp.groups = h.d_sr_groups + h.sr_group_off[s];
+      lp.nodes = h.d_sr_nodes + h.sr_node_off[s];
+      lp.leafval = ctx->leafval.ptr;
+      lp.ngroups = ng;
+      lp.nslot_prev = s + 1 < n ? std::max(h.sr_nslot[s + 1], 1) : 1;
+      lp.nslot_cur = std::max(h.sr_nslot[s], 1);
+      lp.nleaf_total = nleaf;
+      lp.n = n;
+      lp.s = s;
+      lp.suffix = 1;
+      launch_level_variant(variant == LV_MMA3PF4 ? LV_MMA3PF4 : LV_MMAPF4, lp, ng, B, st);
+      CUDA_TRY(ctx, cudaGetLastError());
+    }
+  }
   cplx *envs[2] = {ctx->env0.ptr, ctx->env1.ptr};
-  for (int s = 0; s < n; ++s) {
+  for (int s = 0; s < top; ++s) {
     const int ng = h.group_off[s + 1] - h.group_off[s];
     if (ng == 0) break;
     LevelParams lp{};
@@ -759,8 +843,8 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.right = ctx->right.ptr;
     lp.env_prev = envs[(s + 1) & 1];
     lp.env_cur = envs[s & 1];
-    lp.groups = h.d_groups + h.group_off[s];
-    lp.nodes = h.d_nodes + h.node_off[s];
+    lp.groups = (split ? h.d_sl_groups : h.d_groups) + h.group_off[s];
+    lp.nodes = (split ? h.d_sl_nodes : h.d_nodes) + h.node_off[s];
     lp.leafval = ctx->leafval.ptr;
     lp.ngroups = ng;
     lp.nslot_prev = s > 0 ? std::max(h.nslot[s - 1], 1) : 1;
@@ -769,6 +853,12 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.n = n;
     lp.s = s;
     launch_level_variant(variant, lp, ng, B, st);
+    CUDA_TRY(ctx, cudaGetLastError());
+  }
+  if (split && h.npairs > 0) {
+    split_combine_kernel<<<dim3((h.npairs + COMBINE_WARPS - 1) / COMBINE_WARPS, B), COMBINE_WARPS * 32, 0, st>>>(
+        envs[(h.cut - 1) & 1], std::max(h.nslot[h.cut - 1], 1), (h.cut & 1) ? ctx->env3.ptr : ctx->env2.ptr,
+        std::max(h.sr_nslot[h.cut], 1), h.d_pairs, h.npairs, ctx->status.ptr, ctx->leafval.ptr, nleaf);
     CUDA_TRY(ctx, cudaGetLastError());
   }
   return VQEMPS_OK;
@@ -815,19 +905,33 @@ static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
 // Trie levels and the energy reduction on the prepared states (needs launch_right first).
 static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
                          double *energies_dev, double *per_term_dev) {
-  const int nleaf = std::max(h.nleaf, 1);
+  const int nleaf = std::max(h.e_nleaf(), 1);
   CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
-  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * h.max_slot * ENV_ELEMS));
-  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * h.max_slot * ENV_ELEMS));
+  const size_t pre_slots = h.cut >= 0 ? h.sl_max_slot : h.max_slot;
+  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * pre_slots * ENV_ELEMS));
+  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * pre_slots * ENV_ELEMS));
+  if (h.cut >= 0) {
+    CUDA_TRY(ctx, ctx->env2.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
+    CUDA_TRY(ctx, ctx->env3.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
+    CUDA_TRY(ctx, ctx->sites_t.ensure((size_t)B * ctx->n * SITE_ELEMS));
+  }
   int variant = LV_SIMT4;
   int rc = pick_variant(ctx, h, B, st, &variant);
   if (rc) return rc;
   rc = run_levels(ctx, h, B, st, variant);
   if (rc) return rc;
-  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h.d_leaf_coef, h.nleaf,
-                                             h.d_term_leaf, h.T, ctx->status.ptr, energies_dev,
+  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h.e_leaf_coef(), h.e_nleaf(),
+                                             h.e_term_leaf(), h.T, ctx->status.ptr, energies_dev,
                                              per_term_dev);
   CUDA_TRY(ctx, cudaGetLastError());
+  return VQEMPS_OK;
+}
+
+// Split evaluation of Hamiltonians loaded afterwards: -1 when it saves work
+// (default), 0 never, 1 always (at the best cut).
+extern "C" int vqemps_set_split_mode(vqemps_ctx *ctx, int mode) {
+  if (!ctx || mode < -1 || mode > 1) return VQEMPS_INVALID;
+  ctx->split_mode = mode;
   return VQEMPS_OK;
 }
 
@@ -903,8 +1007,9 @@ extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *
   rc = launch_levels(ctx, *h, B, st, ctx->energy_stage.ptr, nullptr);
   if (rc) return rc;
   CUDA_TRY(ctx, cudaEventRecord(ev[3], st));
-  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h->d_leaf_coef, h->nleaf, h->d_term_leaf,
-                                             h->T, ctx->status.ptr, ctx->energy_stage.ptr, nullptr);
+  reduce_kernel<<<B, REDUCE_THREADS, 0, st>>>(ctx->leafval.ptr, h->e_leaf_coef(), h->e_nleaf(),
+                                             h->e_term_leaf(), h->T, ctx->status.ptr, ctx->energy_stage.ptr,
+                                             nullptr);
   CUDA_TRY(ctx, cudaGetLastError());
   CUDA_TRY(ctx, cudaEventRecord(ev[4], st));
   CUDA_TRY(ctx, cudaEventSynchronize(ev[4]));
@@ -915,8 +1020,14 @@ extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *
   ms[3] = t[3];
   ms[2] = t[2] - t[3];   // launch_levels includes one reduction
   int nlev = 0;
-  for (int s = 0; s < ctx->n; ++s)
+  const int top = h->cut >= 0 ? h->cut : ctx->n;
+  for (int s = 0; s < top; ++s)
     if (h->group_off[s + 1] > h->group_off[s]) ++nlev;
+  if (h->cut >= 0) {
+    nlev += 1 + (h->npairs > 0 ? 1 : 0);            // transpose + pair closures
+    for (int s = h->cut; s < ctx->n; ++s)
+      if (h->sr_group_off[s + 1] > h->sr_group_off[s]) ++nlev;
+  }
   *launches = 1 + 1 + nlev + 1;
   for (auto &e : ev) cudaEventDestroy(e);
   ctx->last_B = B;

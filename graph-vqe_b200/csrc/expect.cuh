@@ -136,6 +136,10 @@ struct LevelParams {
   // Uneven batches: work items (state, first group, group count) of this level,
   // three ints each, one per CTA (null: state = blockIdx.y, all groups).
   const int32_t *work;
+  // Suffix levels of the split evaluation (prefix-pipeline kernels only): sites
+  // holds transposed site tensors and a group without a parent slot starts from
+  // the identity right environment R_{s+1} instead of the vacuum.
+  int suffix;
 };
 
 struct LevelSmem {
@@ -484,6 +488,40 @@ reduce_multi_kernel(const double *__restrict__ leafval, const double *__restrict
   reduce_body(leafval + (size_t)b * leaf_stride, coef + (size_t)k * leaf_stride, part_nleaf[k],
               term_leaf + (size_t)k * term_stride, part_T[k], status[b] == 0, energies + b,
               per_term ? per_term + (size_t)b * term_stride : nullptr);
+}
+
+// Transposed site tensors for the suffix levels of the split evaluation:
+// out[b][s][c][i][a] = in[b][s][a][i][c].
+__global__ void __launch_bounds__(256)
+transpose_sites_kernel(const cplx *__restrict__ in, int n, cplx *__restrict__ out) {
+  const size_t base = ((size_t)blockIdx.y * n + blockIdx.x) * SITE_ELEMS;
+  for (int e = threadIdx.x; e < SITE_ELEMS; e += 256) {
+    const int a = e >> 5, i = (e >> 4) & 1, c = e & 15;
+    out[base + c * 32 + i * 16 + a] = in[base + e];
+  }
+}
+
+// Pair closures of the split evaluation: leafval[b][leaf] = Re sum L o R for
+// (prefix slot, suffix slot, leaf) triples; one warp per pair.
+constexpr int COMBINE_WARPS = 8;
+__global__ void __launch_bounds__(COMBINE_WARPS * 32)
+split_combine_kernel(const cplx *__restrict__ left, int left_nslot, const cplx *__restrict__ right,
+                     int right_nslot, const int32_t *__restrict__ pairs, int npairs,
+                     const int32_t *__restrict__ status, double *__restrict__ leafval, int nleaf_total) {
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pidx = blockIdx.x * COMBINE_WARPS + warp;
+  if (pidx >= npairs) return;
+  const int ls = pairs[3 * pidx], rs = pairs[3 * pidx + 1], leaf = pairs[3 * pidx + 2];
+  const cplx *L = left + ((size_t)b * left_nslot + ls) * ENV_ELEMS;
+  const cplx *R = right + ((size_t)b * right_nslot + rs) * ENV_ELEMS;
+  double v = 0.0;
+  for (int e = lane; e < ENV_ELEMS; e += 32) {
+    const cplx l = L[e], r = R[e];
+    v += l.x * r.x - l.y * r.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) leafval[(size_t)b * nleaf_total + leaf] = status[b] == 0 ? v : 0.0;
 }
 
 }  // namespace vqemps

@@ -208,7 +208,10 @@ struct LevelMmaPfSmem {
 
 __device__ __forceinline__ void stage_parent_padded(const LevelParams &p, int b, int g, cplx *E, int lane) {
   const DevGroup grp = p.groups[g];
-  if (grp.parent_slot < 0) {
+  if (grp.parent_slot < 0 && p.suffix) {
+    const cplx *src = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) cp_async16(E + (e >> 4) * MMA_E_STRIDE + (e & 15), src + e);
+  } else if (grp.parent_slot < 0) {
     for (int e = lane; e < ENV_ELEMS; e += 32)
       E[(e >> 4) * MMA_E_STRIDE + (e & 15)] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
   } else {

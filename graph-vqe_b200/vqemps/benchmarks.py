@@ -63,6 +63,7 @@ def bench_partitions(reps: int = 10):
         se = vqemps.Engine(0, 16)
         se.set_spec(spec)
         se.set_level_variant("dmma3_pf")
+        se.set_split_mode("off")          # the partition set's prefix plan
         singles.append((se, se.set_hamiltonian(words, coeffs),
                         torch.tensor(x, dtype=torch.float64, device=dev).unsqueeze(0),
                         torch.empty(1, dtype=torch.float64, device=dev)))

@@ -214,10 +214,17 @@ class Engine:
         return None if v.value < 0 else self.LEVEL_VARIANTS[v.value]
 
     def plan_stats(self, ham: Hamiltonian) -> dict:
-        out = (ctypes.c_double * 6)()
+        out = (ctypes.c_double * 10)()
         check(self.ctx, self.lib.vqemps_plan_stats(self.ctx, ham.handle, out), "plan_stats")
-        keys = ("flops", "flops_survey", "node_sites", "groups", "leaves", "max_slots")
+        keys = ("flops", "flops_survey", "node_sites", "groups", "leaves", "max_slots", "cut",
+                "prefix_flops", "prefix_node_sites", "pairs")
         return dict(zip(keys, list(out)))
+
+    def set_split_mode(self, mode):
+        """Split evaluation of Hamiltonians loaded afterwards: None/'auto' (when it
+        saves work), False/'off', True/'on'."""
+        m = {None: -1, "auto": -1, False: 0, "off": 0, True: 1, "on": 1}[mode]
+        check(self.ctx, self.lib.vqemps_set_split_mode(self.ctx, m), "set_split_mode")
 
     # -- helpers -------------------------------------------------------------
     def _theta(self, theta):

@@ -193,11 +193,22 @@ int vqemps_level_variant(vqemps_ctx *ctx, int handle, int B, int *variant);
 int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, int B, double *ms,
                           int *launches, void *stream);
 
-/* Work statistics of a loaded Pauli sum, per state and evaluation: stats[0]
- * FP64 flops as executed, stats[1] the survey count 16 Dl Dr (Dl + Dr) per trie
- * node-site, stats[2] node-sites, stats[3] parent groups, stats[4] leaves,
- * stats[5] largest environment slot count of a level. */
+/* Work statistics of a loaded Pauli sum, per state and evaluation (stats[10]):
+ * [0] FP64 flops of the energy path as executed, [1] the survey count
+ * 16 Dl Dr (Dl + Dr) per node-site of the prefix trie, [2] node-sites as
+ * executed, [3] parent groups, [4] leaves, [5] largest environment slot count of
+ * a level, [6] cut site of the split evaluation (-1: prefix trie only),
+ * [7] / [8] flops / node-sites of the prefix trie alone, [9] prefix/suffix
+ * pairs closed at the cut. */
 int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats);
+
+/* Split evaluation (no reference counterpart; the reference walks prefix tries
+ * only, sharded_mps.cuh:614-687): a Pauli sum loaded afterwards is evaluated as
+ * a prefix trie up to a cut site plus a suffix trie from the cut, each word
+ * closed by one dot product of its prefix and suffix environments when that
+ * needs fewer node-sites. mode -1 (default): when it saves at least 15 % of the
+ * node-sites; 0: never; 1: always, at the best cut. Same values to rounding. */
+int vqemps_set_split_mode(vqemps_ctx *ctx, int mode);
 
 /* Copy the site tensors of state b of the last batched call to the host:
  * n * 16 * 2 * 16 complex (re, im) pairs, site s at offset s * 1024 doubles,

@@ -46,6 +46,7 @@ def _single(vq, spec, words, coeffs, order="msb"):
     eng = vq.Engine(0, 16)
     eng.set_spec(spec, site_order=order)
     eng.set_level_variant("dmma3_pf")
+    eng.set_split_mode("off")            # partition sets run the prefix plan
     return eng, eng.set_hamiltonian(words, coeffs)
 
 

@@ -1,0 +1,90 @@
+"""GPU: split evaluation (prefix trie up to a cut site, suffix trie from it, one
+dot product per prefix/suffix pair) against the prefix trie alone and the
+oracle. Same values to rounding: 1e-12 relative between the two plans, the usual
+1e-9 against the oracle."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import mps_oracle as O
+from oracle import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reverse_mps_golden.json").read_text())
+
+
+@pytest.fixture(scope="module")
+def vq(cuda_device):
+    import vqemps
+    return vqemps
+
+
+def _spec(case):
+    s = case["spec"]
+    return dict(n=s["n"], ops=[tuple(o) for o in s["ops"]], initial=s["initial"], count=s["count"])
+
+
+def _energies(vq, spec, words, coeffs, thetas, mode, variant=None, order="msb"):
+    eng = vq.Engine(0, 16)
+    eng.set_spec(spec, site_order=order)
+    eng.set_split_mode(mode)
+    eng.set_level_variant(variant)
+    ham = eng.set_hamiltonian(words, coeffs)
+    e, pt = eng.energy(ham, thetas, per_term=True)
+    return e.cpu().numpy(), pt.cpu().numpy(), eng.plan_stats(ham)
+
+
+@pytest.mark.parametrize("order", ["msb", "qubit"])
+@pytest.mark.parametrize("case", [c for c in GOLDEN if c["spec"]["n"] >= 3], ids=lambda c: c["name"])
+def test_forced_split_matches_golden_and_prefix_plan(vq, case, order):
+    spec = _spec(case)
+    x = np.array(case["x"])
+    e1, pt1, st1 = _energies(vq, spec, case["words"], case["coeffs"], x, "on", order=order)
+    e0, pt0, st0 = _energies(vq, spec, case["words"], case["coeffs"], x, "off", order=order)
+    assert st1["cut"] >= 1 and st0["cut"] == -1
+    assert abs(e1[0] - case["energy"]) <= 1e-9 * max(1.0, abs(case["energy"]))
+    assert abs(e1[0] - e0[0]) <= 1e-12 * max(1.0, abs(e0[0]))
+    np.testing.assert_allclose(pt1, pt0, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("variant", [None, "simt", "dmma_pf", "dmma3_pf"])
+def test_auto_split_at_40_qubits(vq, variant):
+    """The 40-qubit, 5,000-term plan splits by itself and needs about half the
+    node-sites; every level-kernel variant gives the same energies and per-term
+    values as the prefix plan."""
+    spec, words, coeffs, thetas = W.batched_40q(2, batch=8)
+    words = list(words) + ["I" * 40]                       # an identity word as well
+    coeffs = np.append(coeffs, 3.5)
+    e1, pt1, st1 = _energies(vq, spec, words, coeffs, thetas, "auto", variant)
+    e0, pt0, st0 = _energies(vq, spec, words, coeffs, thetas, "off", variant)
+    assert 1 <= st1["cut"] < 39 and st1["node_sites"] < 0.6 * st1["prefix_node_sites"]
+    assert st1["pairs"] > 0
+    np.testing.assert_allclose(e1, e0, rtol=1e-12)
+    np.testing.assert_allclose(pt1, pt0, rtol=0, atol=1e-11)
+    ref = float(np.dot(O.expect_words(O.svd_evolve(spec, thetas[3], 16), words).real, coeffs))
+    assert abs(e1[3] - ref) <= 1e-9 * max(1.0, abs(ref))
+
+
+def test_split_with_sampling_and_widths(vq):
+    """Shot estimates use the split plan's analytic X/Y values; tiny widths and
+    words ending on either side of the cut."""
+    rng = np.random.default_rng(5)
+    from oracle.workloads import random_hamiltonian
+    for n in (3, 4, 9):
+        spec = O.hardware_efficient_spec(n, 3, ("ry", "rz"), "linear")
+        words, coeffs = random_hamiltonian(rng, n, 40, 3, z_fraction=0.6)
+        words[0] = "I" * n
+        x = rng.uniform(-np.pi, np.pi, spec["count"])
+        out = {}
+        for mode in ("on", "off"):
+            eng = vq.Engine(0, 16)
+            eng.set_spec(spec)
+            eng.set_split_mode(mode)
+            ham = eng.set_hamiltonian(words, coeffs)
+            e, pt = eng.sampled_energy(ham, x, 500, 11, "philox", "shared", per_term=True)
+            out[mode] = (e.cpu().numpy(), pt.cpu().numpy(), eng.plan_stats(ham)["cut"])
+        assert out["on"][2] >= 1
+        np.testing.assert_allclose(out["on"][1], out["off"][1], rtol=0, atol=1e-12)
+        np.testing.assert_allclose(out["on"][0], out["off"][0], rtol=1e-12, atol=1e-12)

@@ -38,6 +38,7 @@ def test_batched_local_solves_equal_sequential_solves(vq):
         se = vq.Engine(0, 16)
         se.set_circuit(m["width"], m["ops"], site_order="msb")
         se.set_level_variant("dmma3_pf")
+        se.set_split_mode("off")          # the partition set's plan
         h = se.set_hamiltonian([t for t, _ in m["terms"]], [c for _, c in m["terms"]])
         energies = lambda X: se.energy(h, torch.as_tensor(X, device=se.device)).cpu().numpy()  # noqa: E731
         seq = minimize_model(theta[m["parameter_indices"]], 6, m["constant"], energies, None,
