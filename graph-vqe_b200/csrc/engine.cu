@@ -100,6 +100,53 @@ struct Hamiltonian {
   const int32_t *e_term_leaf() const { return cut >= 0 ? d_split_term_leaf : d_term_leaf; }
 };
 
+// As-soon-as-possible schedule of a circuit's two-site gates for the two-CTA gate
+// chain (evolve_pair_kernel), at most two gates per step on disjoint site pairs,
+// and the one-site gates each two-site gate folds in (see EvolveParams).
+struct PairSched {
+  std::vector<int32_t> sched, gate_q, qlist, tail_off;
+  int nsteps = 0;
+};
+
+PairSched build_pair_schedule(const std::vector<DevGate> &gates, int n) {
+  PairSched ps;
+  ps.gate_q.assign(4 * std::max<size_t>(gates.size(), 1), 0);
+  std::vector<std::vector<int32_t>> pend(n);
+  std::vector<int> last_step(n, -1), count;
+  for (int gi = 0; gi < (int)gates.size(); ++gi) {
+    const DevGate &g = gates[gi];
+    if (g.kind == GATE_ONE) {
+      pend[g.site].push_back(gi);
+      continue;
+    }
+    const int s = g.site;
+    for (int side = 0; side < 2; ++side) {
+      ps.gate_q[4 * gi + 2 * side] = (int32_t)ps.qlist.size();
+      ps.qlist.insert(ps.qlist.end(), pend[s + side].begin(), pend[s + side].end());
+      ps.gate_q[4 * gi + 2 * side + 1] = (int32_t)ps.qlist.size();
+      pend[s + side].clear();
+    }
+    int t = std::max(last_step[s], last_step[s + 1]) + 1;
+    while (t < (int)count.size() && count[t] >= 2) ++t;
+    if (t == (int)count.size()) {
+      count.push_back(0);
+      ps.sched.push_back(-1);
+      ps.sched.push_back(-1);
+    }
+    ps.sched[2 * t + count[t]] = gi;
+    ++count[t];
+    last_step[s] = last_step[s + 1] = t;
+  }
+  ps.tail_off.resize(n + 1);
+  for (int x = 0; x < n; ++x) {
+    ps.tail_off[x] = (int32_t)ps.qlist.size();
+    ps.qlist.insert(ps.qlist.end(), pend[x].begin(), pend[x].end());
+  }
+  ps.tail_off[n] = (int32_t)ps.qlist.size();
+  ps.nsteps = (int)count.size();
+  return ps;
+}
+
 // A partition set: K independent circuits with their own widths, parameters
 // and Hamiltonians, evaluated together in one batch. Per-partition tables sit
 // at fixed strides (widest partition, most terms, most leaves); the trie
@@ -120,6 +167,10 @@ struct PartSet {
   cplx *d_mats = nullptr;
   DevGroup *d_groups = nullptr;
   DevNode *d_nodes = nullptr;
+  PairSched psched;                 // merged two-CTA schedules
+  std::vector<int32_t> step_off, part_tail_off;
+  int32_t *d_sched = nullptr, *d_step_off = nullptr, *d_gate_q = nullptr, *d_qlist = nullptr;
+  int32_t *d_tail_off = nullptr, *d_part_tail_off = nullptr;
   int32_t *d_part = nullptr;        // part_n | part_T | part_nleaf | part_idleaf | part_gate_off (K+1)
   double *d_leaf_coef = nullptr;    // K x leaf_stride
   int32_t *d_term_leaf = nullptr;   // K x T_max
@@ -135,6 +186,8 @@ struct PartSet {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_part);
     cudaFree(d_leaf_coef); cudaFree(d_term_leaf); cudaFree(d_zmask); cudaFree(d_coeffs);
     cudaFree(d_sumidx); cudaFree(d_st_part); cudaFree(d_work);
+    cudaFree(d_sched); cudaFree(d_step_off); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off);
+    cudaFree(d_part_tail_off);
   }
 };
 
@@ -196,9 +249,14 @@ struct vqemps_ctx {
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
   int grad_mma = 2;                     // gradient levels: 0 SIMT, 1 FP64 DMMA, 2 DMMA with Gauss forward
   int split_mode = -1;                  // split evaluation: -1 when it saves work, 0 never, 1 always
+  int evolve_pair = -1;                 // gate chain: 1 two-CTA clusters, 0 one CTA, -1 by batch size
+  int sm_count = 148;
+  PairSched psched;
+  int32_t *d_sched = nullptr, *d_gate_q = nullptr, *d_qlist = nullptr, *d_tail_off = nullptr;
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
+    cudaFree(d_sched); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off);
   }
 };
 
@@ -237,6 +295,10 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   ctx->abs_cut = abs_cut;
   ctx->rel_cut = rel_cut;
   cudaFuncSetAttribute(evolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(evolve_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (const char *v = std::getenv("VQEMPS_EVOLVE"))
+    ctx->evolve_pair = std::strcmp(v, "chain") == 0 ? 0 : std::strcmp(v, "pair") == 0 ? 1 : -1;
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
   cudaFuncSetAttribute(level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelSmem));
   cudaFuncSetAttribute(level_mma_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -450,6 +512,21 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
   if (!gates.empty())
     CUDA_TRY(ctx, cudaMemcpy(ctx->d_gates, gates.data(), gates.size() * sizeof(DevGate), cudaMemcpyHostToDevice));
   CUDA_TRY(ctx, cudaMemcpy(ctx->d_mats, mats.data(), mats.size() * sizeof(cplx), cudaMemcpyHostToDevice));
+  {
+    PairSched ps = build_pair_schedule(gates, n);
+    auto upi = [&](int32_t *&dst, const std::vector<int32_t> &v) -> cudaError_t {
+      cudaFree(dst);
+      dst = nullptr;
+      cudaError_t e = cudaMalloc(&dst, std::max<size_t>(v.size(), 1) * sizeof(int32_t));
+      if (e == cudaSuccess && !v.empty()) e = cudaMemcpy(dst, v.data(), v.size() * sizeof(int32_t), cudaMemcpyHostToDevice);
+      return e;
+    };
+    CUDA_TRY(ctx, upi(ctx->d_sched, ps.sched));
+    CUDA_TRY(ctx, upi(ctx->d_gate_q, ps.gate_q));
+    CUDA_TRY(ctx, upi(ctx->d_qlist, ps.qlist));
+    CUDA_TRY(ctx, upi(ctx->d_tail_off, ps.tail_off));
+    ctx->psched = std::move(ps);
+  }
   ctx->gates = std::move(gates);
   ctx->mats = std::move(mats);
   ctx->grad_ops = std::move(gops);
@@ -733,6 +810,14 @@ static int ensure_state_ws(vqemps_ctx *ctx, int B) {
   return VQEMPS_OK;
 }
 
+// Two-CTA gate chains halve the chain's critical path but double the CTAs: they
+// pay while every state's pair of CTAs finds room next to the others (measured on
+// B200 at 40 qubits: 1.3x faster at B <= 128, slower at B = 256), so by default
+// they run while B is at most the SM count.
+static bool use_pair_chain(const vqemps_ctx *ctx, int B) {
+  return ctx->evolve_pair > 0 || (ctx->evolve_pair < 0 && B <= ctx->sm_count);
+}
+
 static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaStream_t st) {
   EvolveParams ep{};
   ep.gates = ctx->d_gates;
@@ -749,7 +834,16 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
   ep.max_bond = ctx->max_bond;
   ep.abs_cut = ctx->abs_cut;
   ep.rel_cut = ctx->rel_cut;
-  evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+  if (use_pair_chain(ctx, B)) {
+    ep.sched = ctx->d_sched;
+    ep.nsteps = ctx->psched.nsteps;
+    ep.gate_q = ctx->d_gate_q;
+    ep.qlist = ctx->d_qlist;
+    ep.tail_off = ctx->d_tail_off;
+    evolve_pair_kernel<<<2 * B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+  } else {
+    evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+  }
   CUDA_TRY(ctx, cudaGetLastError());
   return VQEMPS_OK;
 }
@@ -924,6 +1018,15 @@ static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st
                                              h.e_term_leaf(), h.T, ctx->status.ptr, energies_dev,
                                              per_term_dev);
   CUDA_TRY(ctx, cudaGetLastError());
+  return VQEMPS_OK;
+}
+
+// Gate chain: 1 two-CTA clusters on an as-soon-as-possible schedule, 0 one CTA
+// in program order, -1 (default) two-CTA clusters while B <= the SM count.
+// Same states bit for bit.
+extern "C" int vqemps_set_evolve_mode(vqemps_ctx *ctx, int mode) {
+  if (!ctx || mode < -1 || mode > 1) return VQEMPS_INVALID;
+  ctx->evolve_pair = mode;
   return VQEMPS_OK;
 }
 

@@ -24,6 +24,8 @@
 // singular value is numerically zero. Singular values are kept in descending
 // order, the gesvd ordering the reference uses.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace vqemps {
@@ -61,6 +63,19 @@ struct EvolveParams {
   const int32_t *st_part;
   const int32_t *part_n;
   const int32_t *part_gate_off;
+  // Two-CTA schedule (evolve_pair_kernel): step t applies gates sched[2t] and
+  // sched[2t + 1] (-1: none) on disjoint site pairs; gate_q[4g .. 4g + 3] bounds
+  // the pending one-site gates (qlist) folded into two-site gate g on its left
+  // and right site; tail_off[x .. x + 1] the one-site gates after the last
+  // two-site gate on site x. Partition sets: steps step_off[k] .. step_off[k + 1]
+  // and tail entries from part_tail_off[k].
+  const int32_t *sched;
+  int nsteps;
+  const int32_t *step_off;
+  const int32_t *gate_q;
+  const int32_t *qlist;
+  const int32_t *tail_off;
+  const int32_t *part_tail_off;
 };
 
 constexpr int EVOLVE_THREADS = 256;
@@ -99,66 +114,48 @@ __device__ __forceinline__ void one_site_matrix(const DevGate &g, const cplx *ma
   }
 }
 
-__global__ void __launch_bounds__(EVOLVE_THREADS)
-evolve_kernel(EvolveParams p) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
-  cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
-  cplx *SA = reinterpret_cast<cplx *>(smem + EvolveSmem::SA);
-  cplx *SB = reinterpret_cast<cplx *>(smem + EvolveSmem::SB);
-  cplx *G = reinterpret_cast<cplx *>(smem + EvolveSmem::G);
-  double *NORM = reinterpret_cast<double *>(smem + EvolveSmem::NORM);
-  double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
-  int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
-  int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
-  cplx *PEND = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);
-  int *BOND = reinterpret_cast<int *>(smem + EvolveSmem::PEND + p.n * 4 * 16);
+// u <- m u for 2 x 2 matrices (a one-site gate joining the pending product).
+// Not inlined, so that both gate chains round it identically.
+__device__ __noinline__ void left_multiply_2x2(const cplx *m, cplx *u) {
+  const cplx u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
+  u[0] = cadd(cmul(m[0], u0), cmul(m[1], u2));
+  u[1] = cadd(cmul(m[0], u1), cmul(m[1], u3));
+  u[2] = cadd(cmul(m[2], u0), cmul(m[3], u2));
+  u[3] = cadd(cmul(m[2], u1), cmul(m[3], u3));
+}
 
+// a[l, i, r] <- sum_j u[i][j] a[l, j, r] for the entries e = tid, tid + step, ...
+// of one site (a one-site matrix applied in place). Not inlined, as above.
+__device__ __noinline__ void apply_2x2_to_site(const cplx *u, cplx *a, int tid, int step) {
+  for (int e = tid; e < CHI * CHI; e += step) {
+    const int l = e >> 4, r = e & 15;
+    const cplx a0 = __ldcg(a + (l * 2 + 0) * CHI + r), a1 = __ldcg(a + (l * 2 + 1) * CHI + r);
+    a[(l * 2 + 0) * CHI + r] = cadd(cmul(u[0], a0), cmul(u[1], a1));
+    a[(l * 2 + 1) * CHI + r] = cadd(cmul(u[2], a0), cmul(u[3], a1));
+  }
+}
+
+// One two-site gate on sites (s, s + 1) of one state, by the whole CTA: Theta =
+// G (U_s (x) U_{s+1}) (A_s A_{s+1}), FP64 one-sided Jacobi SVD, rank selection and
+// the packed factors written back to sites_b. us / ut: the pending one-site
+// matrices of the two sites (reset to the identity here); gm: the 4 x 4 gate.
+// Writes the new bond dimension to *bond_next; returns the status (uniform over
+// the CTA; MISC[0] holds it too).
+struct EvolveShared {
+  cplx *X, *VT, *SA, *SB, *G;
+  double *NORM, *SIG;
+  int *PERM, *MISC;
+};
+
+__device__ __forceinline__ int two_site_update(const EvolveParams &p, const EvolveShared &sh, cplx *sites_b, int s,
+                                            int dl, int dc, int dr, cplx *us, cplx *ut, const cplx *gm,
+                                            int *bond_next) {
+  cplx *X = sh.X, *VT = sh.VT, *SA = sh.SA, *SB = sh.SB, *G = sh.G;
+  double *NORM = sh.NORM, *SIG = sh.SIG;
+  int *PERM = sh.PERM, *MISC = sh.MISC;
   const int tid = threadIdx.x;
-  const int b = blockIdx.x;
-  const int part = p.st_part ? p.st_part[b] : 0;
-  const int n = p.st_part ? p.part_n[part] : p.n;
-  const int gate_begin = p.st_part ? p.part_gate_off[part] : 0;
-  const int gate_end = p.st_part ? p.part_gate_off[part + 1] : p.ngates;
-  const double *theta_b = p.theta + (size_t)b * p.P;
-  cplx *sites_b = p.sites + (size_t)b * p.n * SITE_ELEMS;
-
-  // |init>^n product state, zero padded; identity pending matrices.
-  for (int e = tid; e < n * SITE_ELEMS; e += EVOLVE_THREADS) {
-    int el = e % SITE_ELEMS;
-    cplx v = cmake(0, 0);
-    if (el == 0) v = p.init0;
-    else if (el == CHI) v = p.init1;   // (l=0, p=1, r=0)
-    sites_b[e] = v;
-  }
-  for (int s = tid; s < n; s += EVOLVE_THREADS) {
-    PEND[s * 4 + 0] = cmake(1, 0); PEND[s * 4 + 1] = cmake(0, 0);
-    PEND[s * 4 + 2] = cmake(0, 0); PEND[s * 4 + 3] = cmake(1, 0);
-  }
-  for (int s = tid; s <= n; s += EVOLVE_THREADS) BOND[s] = 1;
-  if (tid == 0) MISC[0] = ST_OK;
-  __syncthreads();
-
   const double eps = 2.2204460492503131e-16;
-  for (int gi = gate_begin; gi < gate_end; ++gi) {
-    const DevGate g = p.gates[gi];
-    if (g.kind == GATE_ONE) {
-      if (tid == 0) {
-        cplx m[4];
-        one_site_matrix(g, p.mats, theta_b, m);
-        cplx *u = PEND + g.site * 4;
-        cplx u0 = u[0], u1 = u[1], u2 = u[2], u3 = u[3];
-        u[0] = cadd(cmul(m[0], u0), cmul(m[1], u2));
-        u[1] = cadd(cmul(m[0], u1), cmul(m[1], u3));
-        u[2] = cadd(cmul(m[2], u0), cmul(m[3], u2));
-        u[3] = cadd(cmul(m[2], u1), cmul(m[3], u3));
-      }
-      __syncthreads();
-      continue;
-    }
     // ---- two-site gate on (s, s+1) ----
-    const int s = g.site;
-    const int dl = BOND[s], dc = BOND[s + 1], dr = BOND[s + 2];
     const int m = 2 * dl, ncol = 2 * dr;
     // Jacobi runs on the shorter side: the rows of Theta when m <= ncol, the
     // rows of Theta^T (the columns of Theta) when Theta is tall.
@@ -167,24 +164,22 @@ evolve_kernel(EvolveParams p) {
     {
       const cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       const cplx *gb = ga + SITE_ELEMS;
-      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) { SA[e] = ga[e]; SB[e] = gb[e]; }
+      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) { SA[e] = __ldcg(ga + e); SB[e] = __ldcg(gb + e); }
       if (tid < 16) {
         // G' = G (U_s (x) U_{s+1}); G'[IJ, ij] = sum_{i'j'} G[IJ, i'j'] U_s[i', i] U_{s+1}[j', j]
         const int row = tid >> 2, col = tid & 3;
         const int i = col >> 1, j = col & 1;
-        const cplx *us = PEND + s * 4, *ut = PEND + (s + 1) * 4;
         cplx acc = cmake(0, 0);
         for (int ip = 0; ip < 2; ++ip)
           for (int jp = 0; jp < 2; ++jp)
-            acc = cadd(acc, cmul(p.mats[g.mat + row * 4 + ip * 2 + jp],
-                                 cmul(us[ip * 2 + i], ut[jp * 2 + j])));
+            acc = cadd(acc, cmul(gm[row * 4 + ip * 2 + jp], cmul(us[ip * 2 + i], ut[jp * 2 + j])));
         G[tid] = acc;
       }
     }
     __syncthreads();
     if (tid < 4) {
-      PEND[s * 4 + tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
-      PEND[(s + 1) * 4 + tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+      us[tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+      ut[tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
     }
     // Theta[(l*2+I), (J*dr+r)] = sum_ij G'[(I*2+J)*4+(i*2+j)] sum_c A[l,i,c] B[c,j,r]  (k_buildM)
     double fro = 0.0;
@@ -336,7 +331,7 @@ evolve_kernel(EvolveParams p) {
       MISC[1] = k;
     }
     __syncthreads();
-    if (MISC[0] != ST_OK) break;
+    if (MISC[0] != ST_OK) return MISC[0];
     const int k = MISC[1];
     // ---- pack (left = U_k (Dl,2,k), right = S_k Vh_k (k,2,Dr), packDirectSvdFactors) ----
     if (!tall) {
@@ -399,25 +394,169 @@ evolve_kernel(EvolveParams p) {
         gb[e] = (cc < k && r < dr) ? cscale(VT[PERM[cc] * 32 + (J * dr + r)], SIG[cc]) : cmake(0, 0);
       }
     }
-    if (tid == 0) BOND[s + 1] = k;
+    if (tid == 0) *bond_next = k;
     __syncthreads();
+    return ST_OK;
+}
+
+__global__ void __launch_bounds__(EVOLVE_THREADS)
+evolve_kernel(EvolveParams p) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
+  cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
+  cplx *SA = reinterpret_cast<cplx *>(smem + EvolveSmem::SA);
+  cplx *SB = reinterpret_cast<cplx *>(smem + EvolveSmem::SB);
+  cplx *G = reinterpret_cast<cplx *>(smem + EvolveSmem::G);
+  double *NORM = reinterpret_cast<double *>(smem + EvolveSmem::NORM);
+  double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
+  int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
+  int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
+  cplx *PEND = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);
+  int *BOND = reinterpret_cast<int *>(smem + EvolveSmem::PEND + p.n * 4 * 16);
+
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x;
+  const int part = p.st_part ? p.st_part[b] : 0;
+  const int n = p.st_part ? p.part_n[part] : p.n;
+  const int gate_begin = p.st_part ? p.part_gate_off[part] : 0;
+  const int gate_end = p.st_part ? p.part_gate_off[part + 1] : p.ngates;
+  const double *theta_b = p.theta + (size_t)b * p.P;
+  cplx *sites_b = p.sites + (size_t)b * p.n * SITE_ELEMS;
+
+  // |init>^n product state, zero padded; identity pending matrices.
+  for (int e = tid; e < n * SITE_ELEMS; e += EVOLVE_THREADS) {
+    int el = e % SITE_ELEMS;
+    cplx v = cmake(0, 0);
+    if (el == 0) v = p.init0;
+    else if (el == CHI) v = p.init1;   // (l=0, p=1, r=0)
+    sites_b[e] = v;
+  }
+  for (int s = tid; s < n; s += EVOLVE_THREADS) {
+    PEND[s * 4 + 0] = cmake(1, 0); PEND[s * 4 + 1] = cmake(0, 0);
+    PEND[s * 4 + 2] = cmake(0, 0); PEND[s * 4 + 3] = cmake(1, 0);
+  }
+  for (int s = tid; s <= n; s += EVOLVE_THREADS) BOND[s] = 1;
+  if (tid == 0) MISC[0] = ST_OK;
+  __syncthreads();
+
+  for (int gi = gate_begin; gi < gate_end; ++gi) {
+    const DevGate g = p.gates[gi];
+    if (g.kind == GATE_ONE) {
+      if (tid == 0) {
+        cplx m[4];
+        one_site_matrix(g, p.mats, theta_b, m);
+        left_multiply_2x2(m, PEND + g.site * 4);
+      }
+      __syncthreads();
+      continue;
+    }
+    const int s = g.site;
+    const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC};
+    if (two_site_update(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4, PEND + (s + 1) * 4,
+                        p.mats + g.mat, BOND + s + 1) != ST_OK)
+      break;
   }
   const int status = MISC[0];
   if (status == ST_OK) {
     // apply the still-pending one-site matrices in place (apply1q)
-    for (int s = 0; s < n; ++s) {
-      const cplx u0 = PEND[s * 4 + 0], u1 = PEND[s * 4 + 1], u2 = PEND[s * 4 + 2], u3 = PEND[s * 4 + 3];
-      cplx *a = sites_b + (size_t)s * SITE_ELEMS;
-      for (int e = tid; e < CHI * CHI; e += EVOLVE_THREADS) {
-        const int l = e >> 4, r = e & 15;
-        cplx a0 = a[(l * 2 + 0) * CHI + r], a1 = a[(l * 2 + 1) * CHI + r];
-        a[(l * 2 + 0) * CHI + r] = cadd(cmul(u0, a0), cmul(u1, a1));
-        a[(l * 2 + 1) * CHI + r] = cadd(cmul(u2, a0), cmul(u3, a1));
-      }
-    }
+    for (int s = 0; s < n; ++s) apply_2x2_to_site(PEND + s * 4, sites_b + (size_t)s * SITE_ELEMS, tid, EVOLVE_THREADS);
   }
   for (int s = tid; s <= n; s += EVOLVE_THREADS) p.bonds[(size_t)b * (p.n + 1) + s] = BOND[s];
   if (tid == 0) p.status[b] = status;
+}
+
+// 2 x 2 product of the one-site gates qlist[q0 .. q1) in program order (later
+// gates on the left).
+__device__ __forceinline__ void pending_product(const EvolveParams &p, const double *theta_b, int q0, int q1,
+                                                cplx *u) {
+  u[0] = cmake(1, 0); u[1] = cmake(0, 0); u[2] = cmake(0, 0); u[3] = cmake(1, 0);
+  for (int q = q0; q < q1; ++q) {
+    cplx m[4];
+    one_site_matrix(p.gates[p.qlist[q]], p.mats, theta_b, m);
+    left_multiply_2x2(m, u);
+  }
+}
+
+// The gate chain of one state on a cluster of two CTAs. Two-site gates on
+// disjoint site pairs commute, so a precomputed as-soon-as-possible schedule of
+// at most two gates per step (one per CTA) replaces program order; each step
+// ends with one cluster barrier. Every gate runs the same code on the same data
+// as in evolve_kernel (pending one-site gates folded in the same order), so the
+// state is bit-for-bit the sequential one. Site tensors and bond dimensions live
+// in global memory (read past L1 with ld.global.cg, since the other CTA writes
+// them). Both CTAs take every step, whatever the status, so the barrier counts
+// always match; after a failure the remaining gates are skipped.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EVOLVE_THREADS)
+evolve_pair_kernel(EvolveParams p) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem[];
+  cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
+  cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
+  cplx *SA = reinterpret_cast<cplx *>(smem + EvolveSmem::SA);
+  cplx *SB = reinterpret_cast<cplx *>(smem + EvolveSmem::SB);
+  cplx *G = reinterpret_cast<cplx *>(smem + EvolveSmem::G);
+  double *NORM = reinterpret_cast<double *>(smem + EvolveSmem::NORM);
+  double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
+  int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
+  int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
+  cplx *U = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);     // 8 entries: U_s, U_{s+1}
+
+  const int tid = threadIdx.x;
+  const int rank = (int)cluster.block_rank();
+  const int b = blockIdx.x >> 1;
+  const int part = p.st_part ? p.st_part[b] : 0;
+  const int n = p.st_part ? p.part_n[part] : p.n;
+  const double *theta_b = p.theta + (size_t)b * p.P;
+  cplx *sites_b = p.sites + (size_t)b * p.n * SITE_ELEMS;
+  int32_t *bonds_b = p.bonds + (size_t)b * (p.n + 1);
+  volatile int32_t *status_b = p.status + b;
+
+  // |init>^n product state and unit bonds, split between the two CTAs
+  for (int e = tid + rank * EVOLVE_THREADS; e < n * SITE_ELEMS; e += 2 * EVOLVE_THREADS) {
+    const int el = e % SITE_ELEMS;
+    cplx v = cmake(0, 0);
+    if (el == 0) v = p.init0;
+    else if (el == CHI) v = p.init1;
+    sites_b[e] = v;
+  }
+  for (int x = tid + rank * EVOLVE_THREADS; x <= n; x += 2 * EVOLVE_THREADS) bonds_b[x] = 1;
+  if (rank == 0 && tid == 0) *status_b = ST_OK;
+  __threadfence();
+  cluster.sync();
+
+  const int t0 = p.step_off ? p.step_off[part] : 0;
+  const int t1 = p.step_off ? p.step_off[part + 1] : p.nsteps;
+  const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC};
+  for (int t = t0; t < t1; ++t) {
+    const int gi = p.sched[2 * t + rank];
+    // the other CTA may be writing the status of this step: one vote per CTA
+    const bool ok = __syncthreads_and(*status_b == ST_OK);
+    if (gi >= 0 && ok) {
+      const DevGate g = p.gates[gi];
+      if (tid == 0) {
+        pending_product(p, theta_b, p.gate_q[4 * gi + 0], p.gate_q[4 * gi + 1], U);
+        pending_product(p, theta_b, p.gate_q[4 * gi + 2], p.gate_q[4 * gi + 3], U + 4);
+      }
+      __syncthreads();
+      const int s = g.site;
+      const int dl = __ldcg(bonds_b + s), dc = __ldcg(bonds_b + s + 1), dr = __ldcg(bonds_b + s + 2);
+      const int st = two_site_update(p, sh, sites_b, s, dl, dc, dr, U, U + 4, p.mats + g.mat, bonds_b + s + 1);
+      if (st != ST_OK && tid == 0) *status_b = st;
+    }
+    __threadfence();
+    cluster.sync();
+  }
+  // one-site gates after the last two-site gate on each site (sites split by parity)
+  if (__syncthreads_and(*status_b == ST_OK)) {
+    const int base = p.part_tail_off ? p.part_tail_off[part] : 0;
+    for (int x = rank; x < n; x += 2) {
+      __syncthreads();
+      if (tid == 0) pending_product(p, theta_b, p.tail_off[base + x], p.tail_off[base + x + 1], U);
+      __syncthreads();
+      apply_2x2_to_site(U, sites_b + (size_t)x * SITE_ELEMS, tid, EVOLVE_THREADS);
+    }
+  }
 }
 
 }  // namespace vqemps

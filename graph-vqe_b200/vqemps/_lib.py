@@ -28,7 +28,8 @@ SYMBOLS = (
     "vqemps_batch_status", "vqemps_energy_grad_batch", "vqemps_sample",
     "vqemps_sampled_energy", "vqemps_copy_sites", "vqemps_plan_stats", "vqemps_profile_energy",
     "vqemps_energy_noalloc", "vqemps_set_level_variant", "vqemps_level_variant",
-    "vqemps_set_grad_checkpoint", "vqemps_set_grad_variant", "vqemps_set_split_mode", "vqemps_set_partitions", "vqemps_free_partitions",
+    "vqemps_set_grad_checkpoint", "vqemps_set_grad_variant", "vqemps_set_split_mode", "vqemps_set_evolve_mode",
+    "vqemps_set_partitions", "vqemps_free_partitions",
     "vqemps_partition_info", "vqemps_partition_bond_dims", "vqemps_partition_energy",
     "vqemps_partition_sample", "vqemps_partition_sampled_energy",
     "vqemps_mpnn_create", "vqemps_mpnn_destroy", "vqemps_mpnn_last_error", "vqemps_mpnn_num_params",
@@ -95,6 +96,7 @@ def load():
         "vqemps_set_grad_checkpoint": (I, [P, I]),
         "vqemps_set_grad_variant": (I, [P, I]),
         "vqemps_set_split_mode": (I, [P, I]),
+        "vqemps_set_evolve_mode": (I, [P, I]),
         "vqemps_level_variant": (I, [P, I, I, ctypes.POINTER(I)]),
         "vqemps_set_partitions": (I, [P, I, V, ctypes.POINTER(VqempsOp), V, V, V, ctypes.c_char_p, V, V,
                                       I, I, ctypes.POINTER(I)]),

@@ -220,6 +220,12 @@ class Engine:
                 "prefix_flops", "prefix_node_sites", "pairs")
         return dict(zip(keys, list(out)))
 
+    def set_evolve_mode(self, mode: str):
+        """Gate chain: 'pair' (two-CTA clusters on a schedule), 'chain' (one CTA, program
+        order) or 'auto' (pair while the batch has at most one state per SM; default)."""
+        check(self.ctx, self.lib.vqemps_set_evolve_mode(self.ctx, {"chain": 0, "pair": 1, "auto": -1}[mode]),
+              "set_evolve_mode")
+
     def set_split_mode(self, mode):
         """Split evaluation of Hamiltonians loaded afterwards: None/'auto' (when it
         saves work), False/'off', True/'on'."""
