@@ -86,12 +86,18 @@ struct Hamiltonian {
   DevNode *d_sl_nodes = nullptr, *d_sr_nodes = nullptr;
   int32_t *d_pairs = nullptr, *d_split_term_leaf = nullptr;
   double *d_split_leaf_coef = nullptr;
+  // Pair cotangents of the split gradient, summed in a fixed order: the pairs of
+  // prefix slot j are pl_off[j] .. pl_off[j+1]-1 (pairs are sorted by prefix
+  // slot); those of suffix slot r are pr_idx[pr_off[r] .. pr_off[r+1]-1].
+  std::vector<int32_t> pl_off, pr_off, pr_idx;
+  int32_t *d_pl_off = nullptr, *d_pr_off = nullptr, *d_pr_idx = nullptr;
   ~Hamiltonian() {
     cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_leaf_coef); cudaFree(d_term_leaf);
     cudaFree(d_zmask); cudaFree(d_offdiag); cudaFree(d_codes); cudaFree(d_coeffs);
     cudaFree(d_sumidx_shared); cudaFree(d_sumidx_word); cudaFree(d_wordlist);
     cudaFree(d_sl_groups); cudaFree(d_sr_groups); cudaFree(d_sl_nodes); cudaFree(d_sr_nodes);
     cudaFree(d_pairs); cudaFree(d_split_term_leaf); cudaFree(d_split_leaf_coef);
+    cudaFree(d_pl_off); cudaFree(d_pr_off); cudaFree(d_pr_idx);
   }
   // leaves of the energy path (split plan when cut >= 0)
   int e_nleaf() const { return cut >= 0 ? split_nleaf : nleaf; }
@@ -243,6 +249,9 @@ struct vqemps_ctx {
   DevBuf<cplx> branch;
   DevBuf<double> analytic_stage;
   DevBuf<cplx> grad_sites, grad_envs, grad_seg, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
+  // split gradient: transposed sites, suffix environments (all levels), suffix
+  // cotangents (ping-pong), cotangents of R_{s+1} from the suffix roots
+  DevBuf<cplx> grad_sites_t, grad_senv, grad_sbar0, grad_sbar1, grad_rootbar;
   DevBuf<double> grad_stage;
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
@@ -345,6 +354,8 @@ extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
   ctx->grad_sites.release(); ctx->grad_envs.release(); ctx->grad_bar0.release();
   ctx->grad_bar1.release(); ctx->grad_sitebar.release(); ctx->grad_stage.release();
   ctx->grad_partial.release(); ctx->grad_leafsum.release(); ctx->grad_seg.release();
+  ctx->grad_sites_t.release(); ctx->grad_senv.release(); ctx->grad_sbar0.release();
+  ctx->grad_sbar1.release(); ctx->grad_rootbar.release();
   delete ctx;
   return VQEMPS_OK;
 }
@@ -761,6 +772,9 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
     CUDA_TRY(ctx, up(h->d_pairs, h->pairs));
     CUDA_TRY(ctx, up(h->d_split_leaf_coef, h->split_leaf_coef));
     CUDA_TRY(ctx, up(h->d_split_term_leaf, h->split_term_leaf));
+    CUDA_TRY(ctx, up(h->d_pl_off, h->pl_off));
+    CUDA_TRY(ctx, up(h->d_pr_off, h->pr_off));
+    CUDA_TRY(ctx, up(h->d_pr_idx, h->pr_idx));
   }
   const int id = ctx->next_handle++;
   ctx->hams[id] = std::move(h);

@@ -174,6 +174,12 @@ struct GradLevelParams {
   const cplx *bar_cur;      // backward: cotangents of level s slots
   int maxslot;
   int ngroups, n, s;
+  // Suffix levels of the split evaluation (DMMA kernels only): sites holds the
+  // transposed site tensors, a group without a parent slot starts from the
+  // identity right environment R_{s+1}, and the backward writes that group's
+  // parent cotangent (the cotangent of R_{s+1}) to rootbar[b][s].
+  int suffix;
+  cplx *rootbar;            // B x n x ENV_ELEMS
 };
 
 struct GradFwdSmem {
@@ -325,14 +331,61 @@ __global__ void partial_sum_kernel(const cplx *__restrict__ partial, int parts, 
   out[(size_t)b * out_stride + e] = acc;
 }
 
+// out[b][a][i][c] += sum over parts of partial[b][part][c][i][a], fixed order:
+// site cotangents of the split evaluation's suffix levels (transposed sites).
+__global__ void partial_sum_t_kernel(const cplx *__restrict__ partial, int parts, cplx *__restrict__ out,
+                                     size_t out_stride) {
+  const int b = blockIdx.y;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= SITE_ELEMS) return;
+  const int a = e >> 5, i = (e >> 4) & 1, c = e & 15;
+  const cplx *src = partial + (size_t)b * parts * SITE_ELEMS + c * 32 + i * 16 + a;
+  cplx acc = out[(size_t)b * out_stride + e];
+  for (int k = 0; k < parts; ++k) acc = cadd(acc, src[(size_t)k * SITE_ELEMS]);
+  out[(size_t)b * out_stride + e] = acc;
+}
+
+// Cotangents of the split evaluation's pair closures <P> = Re sum L o R with
+// weight c (the pair's leaf coefficient): Lbar[j] = sum_p c_p conj(R[rs_p]) over
+// the pairs of prefix slot j, Rbar[r] = sum_p c_p conj(L[ls_p]) over those of
+// suffix slot r, each in pair order. Block (slot, state), thread per element.
+__global__ void __launch_bounds__(ENV_ELEMS)
+split_pair_bwd_kernel(const cplx *__restrict__ left, size_t left_stride, const cplx *__restrict__ right,
+                      size_t right_stride, const int32_t *__restrict__ pairs, const double *__restrict__ coef,
+                      const int32_t *__restrict__ pl_off, int nls, const int32_t *__restrict__ pr_off,
+                      const int32_t *__restrict__ pr_idx, cplx *__restrict__ lbar, size_t lbar_stride,
+                      cplx *__restrict__ rbar, size_t rbar_stride) {
+  const int b = blockIdx.y, e = threadIdx.x;
+  const int j = blockIdx.x;
+  cplx acc = cmake(0, 0);
+  if (j < nls) {
+    for (int k = pl_off[j]; k < pl_off[j + 1]; ++k) {
+      const cplx r = right[(size_t)b * right_stride + (size_t)pairs[3 * k + 1] * ENV_ELEMS + e];
+      acc = cadd(acc, cscale(cconj(r), coef[pairs[3 * k + 2]]));
+    }
+    lbar[(size_t)b * lbar_stride + (size_t)j * ENV_ELEMS + e] = acc;
+  } else {
+    const int r = j - nls;
+    for (int q = pr_off[r]; q < pr_off[r + 1]; ++q) {
+      const int k = pr_idx[q];
+      const cplx l = left[(size_t)b * left_stride + (size_t)pairs[3 * k] * ENV_ELEMS + e];
+      acc = cadd(acc, cscale(cconj(l), coef[pairs[3 * k + 2]]));
+    }
+    rbar[(size_t)b * rbar_stride + (size_t)r * ENV_ELEMS + e] = acc;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // suffix part: F_0 = c_identity e00; Abar_q,i = 2 F_q A_q,i conj(R_{q+1});
 // F_{q+1} = sum_i A_i^H F_q A_i + leafsum[q].  One CTA per state.
 // ---------------------------------------------------------------------------
+// rootbar (may be null): cotangents of R_{q+1} from the split evaluation's
+// suffix roots (bar convention, conjugated into F); accumulate adds the site
+// cotangents to sitebar instead of writing them.
 __global__ void __launch_bounds__(256)
 grad_suffix_kernel(const cplx *__restrict__ sites, const cplx *__restrict__ right,
-                   const cplx *__restrict__ leafsum, double identity_coef, int n,
-                   cplx *__restrict__ sitebar) {
+                   const cplx *__restrict__ leafsum, const cplx *__restrict__ rootbar,
+                   double identity_coef, int n, int accumulate, cplx *__restrict__ sitebar) {
   __shared__ cplx A[SITE_ELEMS];
   __shared__ cplx F[ENV_ELEMS];
   __shared__ cplx Rc[ENV_ELEMS];
@@ -359,12 +412,13 @@ grad_suffix_kernel(const cplx *__restrict__ sites, const cplx *__restrict__ righ
       const int ai = e >> 4, c = e & 15;
       cplx acc = cmake(0, 0);
       for (int cp = 0; cp < CHI; ++cp) cfma(acc, Tm[ai * CHI + cp], Rc[cp * CHI + c]);
-      dst[e] = cscale(acc, 2.0);
+      dst[e] = accumulate ? cadd(dst[e], cscale(acc, 2.0)) : cscale(acc, 2.0);
     }
-    // F' = sum_i A_i^H Tm_i + leafsum[q]
+    // F' = sum_i A_i^H Tm_i + leafsum[q] (+ conj(rootbar[q]))
     {
       const int bb = tid >> 4, c = tid & 15;
       cplx acc = leafsum[((size_t)b * n + q) * ENV_ELEMS + tid];
+      if (rootbar) acc = cadd(acc, cconj(rootbar[((size_t)b * n + q) * ENV_ELEMS + tid]));
       for (int a = 0; a < CHI; ++a) {
         cfma_conj(acc, A[(a * 2 + 0) * CHI + bb], Tm[(a * 2 + 0) * CHI + c]);
         cfma_conj(acc, A[(a * 2 + 1) * CHI + bb], Tm[(a * 2 + 1) * CHI + c]);

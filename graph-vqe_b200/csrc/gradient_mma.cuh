@@ -25,7 +25,10 @@ struct GradFwdMmaSmem {
 
 __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int b, int g, cplx *E, int lane) {
   const DevGroup grp = p.groups[g];
-  if (grp.parent_slot < 0) {
+  if (grp.parent_slot < 0 && p.suffix) {
+    const cplx *src = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) cp_async16(E + (e >> 4) * MMA_E_STRIDE + (e & 15), src + e);
+  } else if (grp.parent_slot < 0) {
     for (int e = lane; e < ENV_ELEMS; e += 32)
       E[(e >> 4) * MMA_E_STRIDE + (e & 15)] = cmake(e == 0 ? 1.0 : 0.0, 0.0);
   } else {
@@ -433,7 +436,8 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
             dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
           }
       }
-      cplx *dst = p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS;
+      cplx *dst = grp.parent_slot >= 0 ? p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS
+                                       : p.rootbar + ((size_t)b * p.n + p.s) * ENV_ELEMS;   // suffix root
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll

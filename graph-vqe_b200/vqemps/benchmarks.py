@@ -109,28 +109,35 @@ def bench_partitions(reps: int = 10):
         print(json.dumps(line), flush=True)
 
 
-def bench_gradient(reps: int = 3, every=(8, 1)):
+def bench_gradient(reps: int = 3, every=(8, 1), plans=("auto", "off")):
     spec, words, coeffs, thetas = W.gradient_64q(seed=0)
-    eng = vqemps.Engine(0, 16)
-    eng.set_spec(spec)
-    ham = eng.set_hamiltonian(words, coeffs)
-    dev = eng.device
-    stream = torch.cuda.current_stream(dev)
-    th = torch.tensor(thetas, dtype=torch.float64, device=dev)
-    B = th.shape[0]
-    eng.energy(ham, th)                                    # tunes the level kernel outside the timing
-    for k in every:
-        eng.set_grad_checkpoint(k)
-        free0 = torch.cuda.mem_get_info(dev)[0]
-        eng.energy_grad(ham, th)
-        torch.cuda.synchronize()
-        used = free0 - torch.cuda.mem_get_info(dev)[0]
-        ms = _events_ms(lambda: eng.energy_grad(ham, th), reps, stream)
-        ms_e = _events_ms(lambda: eng.energy(ham, th, check_status=False), reps, stream)
-        print(json.dumps(dict(workload="64q linear RY, 320 angles, 20000 terms (wmax 6), energy + gradient",
-                              batch=B, checkpoint_every=k, ms_per_call=ms, grads_per_s=B / (ms * 1e-3),
-                              energy_only_ms=ms_e, grad_over_energy=ms / ms_e,
-                              workspace_growth_bytes=int(used))), flush=True)
+    for plan in plans:
+        eng = vqemps.Engine(0, 16)
+        eng.set_spec(spec)
+        eng.set_split_mode(plan)
+        ham = eng.set_hamiltonian(words, coeffs)
+        stats = eng.plan_stats(ham)
+        dev = eng.device
+        stream = torch.cuda.current_stream(dev)
+        th = torch.tensor(thetas, dtype=torch.float64, device=dev)
+        B = th.shape[0]
+        eng.energy(ham, th)                                    # tunes the level kernel outside the timing
+        for k in every:
+            eng.set_grad_checkpoint(k)
+            free0 = torch.cuda.mem_get_info(dev)[0]
+            eng.energy_grad(ham, th)
+            torch.cuda.synchronize()
+            used = free0 - torch.cuda.mem_get_info(dev)[0]
+            ms = _events_ms(lambda: eng.energy_grad(ham, th), reps, stream)
+            ms_e = _events_ms(lambda: eng.energy(ham, th, check_status=False), reps, stream)
+            print(json.dumps(dict(workload="64q linear RY, 320 angles, 20000 terms (wmax 6), energy + gradient",
+                                  batch=B, plan="split" if stats["cut"] >= 0 else "prefix", cut=stats["cut"],
+                                  node_sites=stats["node_sites"], checkpoint_every=k, ms_per_call=ms,
+                                  grads_per_s=B / (ms * 1e-3), energy_only_ms=ms_e, grad_over_energy=ms / ms_e,
+                                  workspace_growth_bytes=int(used))), flush=True)
+        eng.close()
+        del th
+        torch.cuda.empty_cache()
 
 
 def bench_graphs(reps: int = 50):
