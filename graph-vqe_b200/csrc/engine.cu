@@ -726,11 +726,14 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
           g.classes |= (c == 0 || c == 3) ? 1 : 2;
         }
         h->groups.push_back(g);
-        // flop accounting with the actual bond dims (dl x dr site)
+        // flop accounting with the actual bond dims (dl x dr site), as the
+        // prefetch DMMA level kernels execute it: the children are Hermitian, so
+        // the I/Z products form three of four output tiles and the X/Y pair one
+        // product (t1 = t0^H)
         const double dl = bd[s], dr = bd[s + 1];
-        const double gf = 8.0 * 2.0 * dl * dl * dr                          // S_i = E A_i
-                          + ((g.classes & 1) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr  // I/Z products
-                          + ((g.classes & 2) ? 1 : 0) * 8.0 * 2.0 * dl * dr * dr; // X/Y products
+        const double gf = 8.0 * 2.0 * dl * dl * dr                                 // S_i = E A_i
+                          + ((g.classes & 1) ? 0.75 : 0.0) * 8.0 * 2.0 * dl * dr * dr  // I/Z products
+                          + ((g.classes & 2) ? 0.5 : 0.0) * 8.0 * 2.0 * dl * dr * dr;  // X/Y product
         h->flops += gf;
         h->level_flops[s] += gf;
         h->flops_survey += (lastn - first + 1) * 16.0 * dl * dr * (dl + dr);

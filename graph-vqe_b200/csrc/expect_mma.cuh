@@ -220,6 +220,58 @@ __device__ __forceinline__ void stage_parent_padded(const LevelParams &p, int b,
   }
 }
 
+// Class-product tiles of conj(A_x)^T S_y (x = column offset 0 or CHI of the A
+// panel, y = panel half) over the 8 x 8 output tiles (rt, ct); SKIP10 leaves
+// the (1,0) tile out. GAUSS: k1 = Yr (Xr - Xi), k2 = Xr (Yi - Yr),
+// k3 = -Xi (Yr + Yi), Re = k1 - k3, Im = k1 + k2; else four real products.
+template <bool GAUSS, bool SKIP10>
+__device__ __forceinline__ void class_tiles(const cplx *A, int xoff, const cplx *S, int y, double (&re)[2][2][2],
+                                            double (&im)[2][2][2], int g, int t) {
+  double k3[2][2][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) re[rt][ct][j] = im[rt][ct][j] = k3[rt][ct][j] = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks) {
+    cplx x[2], yv[2];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt) x[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + xoff + rt * 8 + g];
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct) yv[ct] = S[(y * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct) {
+        if (SKIP10 && rt == 1 && ct == 0) continue;
+        if constexpr (GAUSS) {
+          dmma(re[rt][ct][0], re[rt][ct][1], x[rt].x - x[rt].y, yv[ct].x);
+          dmma(im[rt][ct][0], im[rt][ct][1], x[rt].x, yv[ct].y - yv[ct].x);
+          dmma(k3[rt][ct][0], k3[rt][ct][1], -x[rt].y, yv[ct].x + yv[ct].y);
+        } else {
+          dmma(re[rt][ct][0], re[rt][ct][1], x[rt].x, yv[ct].x);
+          dmma(re[rt][ct][0], re[rt][ct][1], x[rt].y, yv[ct].y);
+          dmma(im[rt][ct][0], im[rt][ct][1], x[rt].x, yv[ct].y);
+          dmma(im[rt][ct][0], im[rt][ct][1], -x[rt].y, yv[ct].x);
+        }
+      }
+  }
+  if constexpr (GAUSS) {
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const double k1 = re[rt][ct][j];
+          re[rt][ct][j] = k1 - k3[rt][ct][j];
+          im[rt][ct][j] = k1 + im[rt][ct][j];
+        }
+  }
+}
+
 // GAUSS selects the complex product: false = four real DMMA products
 // (Re = XrYr - XiYi, Im = XrYi + XiYr); true = Gauss's three-product form
 // k1 = Yr (Xr + Xi), k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi), Re = k1 - k3,
@@ -342,91 +394,35 @@ __device__ __forceinline__ void level_mma_pf_body(const LevelParams &p, int grou
     cp_async_commit();
     for (int cls = 0; cls < 2; ++cls) {
       if (!(grp.classes & (1 << cls))) continue;
-      const int y0 = cls == 0 ? 0 : 1, y1 = cls == 0 ? 1 : 0;
+      // Every trie environment is Hermitian (E' = sum_ij P_ij A_i^H E A_j with P
+      // and the root Hermitian), so the children are too: only the tiles (0,0),
+      // (0,1) and (1,1) are formed, the (1,0) tile is the conjugate transpose of
+      // (0,1). I/Z: t0 = A_0^H S_0 and t1 = A_1^H S_1. X/Y: t0 = A_0^H S_1 (all
+      // four tiles) and t1 = A_1^H S_0 = t0^H, transposed through the S panel.
       double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
-#pragma unroll
-      for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-        for (int ct = 0; ct < 2; ++ct)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) ar[rt][ct][j] = ai[rt][ct][j] = br[rt][ct][j] = bi[rt][ct][j] = 0.0;
-      if constexpr (!GAUSS) {
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-          cplx a0[2], a1[2], s0[2], s1[2];
-#pragma unroll
-          for (int rt = 0; rt < 2; ++rt) {
-            a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
-            a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
-          }
-#pragma unroll
-          for (int ct = 0; ct < 2; ++ct) {
-            s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-            s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-          }
-#pragma unroll
-          for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-            for (int ct = 0; ct < 2; ++ct) {
-              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
-              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
-              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
-              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
-            }
-        }
+      if (cls == 0) {
+        class_tiles<GAUSS, true>(A, 0, S, 0, ar, ai, g, t);
+        class_tiles<GAUSS, true>(A, CHI, S, 1, br, bi, g, t);
       } else {
-        // conj(X) Y with X = A_i, Y = S: k1 = Yr (Xr - Xi), k2 = Xr (Yi - Yr),
-        // k3 = -Xi (Yr + Yi); k1 and k3 accumulate in ar / br (then ar = k1 - k3),
-        // k2 in ai / bi (then ai = k1 + k2)
-        double a3[2][2][2], b3[2][2][2];
+        class_tiles<GAUSS, false>(A, 0, S, 1, ar, ai, g, t);
+        __syncwarp();   // the panel is consumed: t0 goes into its place
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
           for (int ct = 0; ct < 2; ++ct)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) a3[rt][ct][j] = b3[rt][ct][j] = 0.0;
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks) {
-          cplx a0[2], a1[2], s0[2], s1[2];
-#pragma unroll
-          for (int rt = 0; rt < 2; ++rt) {
-            a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
-            a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
-          }
-#pragma unroll
-          for (int ct = 0; ct < 2; ++ct) {
-            s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-            s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-          }
-#pragma unroll
-          for (int rt = 0; rt < 2; ++rt) {
-            const double xd0 = a0[rt].x - a0[rt].y, xd1 = a1[rt].x - a1[rt].y;
-#pragma unroll
-            for (int ct = 0; ct < 2; ++ct) {
-              dmma(ar[rt][ct][0], ar[rt][ct][1], xd0, s0[ct].x);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y - s0[ct].x);
-              dmma(a3[rt][ct][0], a3[rt][ct][1], -a0[rt].y, s0[ct].x + s0[ct].y);
-              dmma(br[rt][ct][0], br[rt][ct][1], xd1, s1[ct].x);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y - s1[ct].x);
-              dmma(b3[rt][ct][0], b3[rt][ct][1], -a1[rt].y, s1[ct].x + s1[ct].y);
-            }
-          }
-        }
+            for (int j = 0; j < 2; ++j)
+              S[(rt * 8 + g) * MMA_S_STRIDE + ct * 8 + 2 * t + j] = cmake(ar[rt][ct][j], ai[rt][ct][j]);
+        __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-          for (int ct = 0; ct < 2; ++ct)
+          for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-              const double k1a = ar[rt][ct][j], k1b = br[rt][ct][j];
-              ar[rt][ct][j] = k1a - a3[rt][ct][j];
-              ai[rt][ct][j] = k1a + ai[rt][ct][j];
-              br[rt][ct][j] = k1b - b3[rt][ct][j];
-              bi[rt][ct][j] = k1b + bi[rt][ct][j];
+              const cplx v = S[(ct * 8 + 2 * t + j) * MMA_S_STRIDE + rt * 8 + g];
+              br[rt][ct][j] = v.x;
+              bi[rt][ct][j] = -v.y;
             }
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
@@ -437,7 +433,7 @@ __device__ __forceinline__ void level_mma_pf_body(const LevelParams &p, int grou
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-          for (int ct = 0; ct < 2; ++ct)
+          for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
               const cplx t0 = cmake(ar[rt][ct][j], ai[rt][ct][j]);
@@ -451,21 +447,28 @@ __device__ __forceinline__ void level_mma_pf_body(const LevelParams &p, int grou
 #pragma unroll
           for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-            for (int ct = 0; ct < 2; ++ct)
+            for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
               for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = cconj(out[0][1][j]);
         }
         if (node.leaf >= 0) {
           double v = 0.0;
 #pragma unroll
           for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-            for (int ct = 0; ct < 2; ++ct)
+            for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
               for (int j = 0; j < 2; ++j) {
                 const cplx rv = R[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j];
                 v += out[rt][ct][j].x * rv.x - out[rt][ct][j].y * rv.y;
               }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {   // the (1,0) tile: Re(conj(o) r)
+            const cplx rv = R[(8 + 2 * t + j) * CHI + g];
+            v += out[0][1][j].x * rv.x + out[0][1][j].y * rv.y;
+          }
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           if (lane == 0) p.leafval[(size_t)b * p.nleaf_total + node.leaf] = v;
         }

@@ -129,72 +129,32 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
     cp_async_commit();
     for (int cls = 0; cls < 2; ++cls) {
       if (!(grp.classes & (1 << cls))) continue;
-      const int y0 = cls == 0 ? 0 : 1, y1 = cls == 0 ? 1 : 0;
+      // Hermitian children: tiles (0,0), (0,1), (1,1) formed, (1,0) = (0,1)^H;
+      // X/Y: t1 = A_1^H S_0 = t0^H through the S panel (as level_mma_pf_body).
       double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
-#pragma unroll
-      for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-        for (int ct = 0; ct < 2; ++ct)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) ar[rt][ct][j] = ai[rt][ct][j] = br[rt][ct][j] = bi[rt][ct][j] = 0.0;
-      double a3[GAUSS ? 2 : 1][2][2], b3[GAUSS ? 2 : 1][2][2];
-      if constexpr (GAUSS) {
+      if (cls == 0) {
+        class_tiles<GAUSS, true>(A, 0, S, 0, ar, ai, g, t);
+        class_tiles<GAUSS, true>(A, CHI, S, 1, br, bi, g, t);
+      } else {
+        class_tiles<GAUSS, false>(A, 0, S, 1, ar, ai, g, t);
+        __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
           for (int ct = 0; ct < 2; ++ct)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) a3[rt][ct][j] = b3[rt][ct][j] = 0.0;
-      }
-#pragma unroll
-      for (int ks = 0; ks < 4; ++ks) {
-        cplx a0[2], a1[2], s0[2], s1[2];
-#pragma unroll
-        for (int rt = 0; rt < 2; ++rt) {
-          a0[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + rt * 8 + g];
-          a1[rt] = A[(ks * 4 + t) * MMA_A_STRIDE + CHI + rt * 8 + g];
-        }
-#pragma unroll
-        for (int ct = 0; ct < 2; ++ct) {
-          s0[ct] = S[(y0 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-          s1[ct] = S[(y1 * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g];
-        }
+            for (int j = 0; j < 2; ++j)
+              S[(rt * 8 + g) * MMA_S_STRIDE + ct * 8 + 2 * t + j] = cmake(ar[rt][ct][j], ai[rt][ct][j]);
+        __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-          for (int ct = 0; ct < 2; ++ct) {
-            if constexpr (GAUSS) {
-              // conj(X) Y: k1 = Yr (Xr - Xi) -> ar, k2 = Xr (Yi - Yr) -> ai, k3 = -Xi (Yr + Yi) -> a3
-              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x - a0[rt].y, s0[ct].x);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y - s0[ct].x);
-              dmma(a3[rt][ct][0], a3[rt][ct][1], -a0[rt].y, s0[ct].x + s0[ct].y);
-              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x - a1[rt].y, s1[ct].x);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y - s1[ct].x);
-              dmma(b3[rt][ct][0], b3[rt][ct][1], -a1[rt].y, s1[ct].x + s1[ct].y);
-            } else {
-              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].x, s0[ct].x);
-              dmma(ar[rt][ct][0], ar[rt][ct][1], a0[rt].y, s0[ct].y);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], a0[rt].x, s0[ct].y);
-              dmma(ai[rt][ct][0], ai[rt][ct][1], -a0[rt].y, s0[ct].x);
-              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].x, s1[ct].x);
-              dmma(br[rt][ct][0], br[rt][ct][1], a1[rt].y, s1[ct].y);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], a1[rt].x, s1[ct].y);
-              dmma(bi[rt][ct][0], bi[rt][ct][1], -a1[rt].y, s1[ct].x);
-            }
-          }
-      }
-      if constexpr (GAUSS) {
-#pragma unroll
-        for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-          for (int ct = 0; ct < 2; ++ct)
+          for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
-              const double k1a = ar[rt][ct][j], k1b = br[rt][ct][j];
-              ar[rt][ct][j] = k1a - a3[rt][ct][j];
-              ai[rt][ct][j] = k1a + ai[rt][ct][j];
-              br[rt][ct][j] = k1b - b3[rt][ct][j];
-              bi[rt][ct][j] = k1b + bi[rt][ct][j];
+              const cplx v = S[(ct * 8 + 2 * t + j) * MMA_S_STRIDE + rt * 8 + g];
+              br[rt][ct][j] = v.x;
+              bi[rt][ct][j] = -v.y;
             }
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
@@ -205,7 +165,7 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-          for (int ct = 0; ct < 2; ++ct)
+          for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
               const cplx t0 = cmake(ar[rt][ct][j], ai[rt][ct][j]);
@@ -214,14 +174,19 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
               else if (node.code == 3) out[rt][ct][j] = csub(t0, t1);
               else { const cplx d = csub(t1, t0); out[rt][ct][j] = cmake(-d.y, d.x); }
             }
+        // out[1][0][j]: the (1,0)-tile element this lane owns, [8 + 2t + j][g]
+        out[1][0][0] = cconj(out[0][1][0]);
+        out[1][0][1] = cconj(out[0][1][1]);
         if (node.env_slot >= 0) {
           cplx *dst = p.env_cur + (size_t)b * p.cur_stride + (size_t)node.env_slot * ENV_ELEMS;
 #pragma unroll
           for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-            for (int ct = 0; ct < 2; ++ct)
+            for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
               for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = out[1][0][j];
         }
         if (node.leaf >= 0 && p.leaf_work) {
           const double cf = p.leaf_coef[node.leaf];
@@ -229,7 +194,7 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
           for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-            for (int ct = 0; ct < 2; ++ct)
+            for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
               for (int j = 0; j < 2; ++j) {
                 const int idx = (rt * 8 + g) * CHI + ct * 8 + 2 * t + j;
@@ -237,6 +202,13 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
                 v += out[rt][ct][j].x * rv.x - out[rt][ct][j].y * rv.y;
                 L[idx] = cadd(L[idx], cscale(out[rt][ct][j], cf));
               }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {   // the (1,0) tile
+            const int idx = (8 + 2 * t + j) * CHI + g;
+            const cplx rv = R[idx];
+            v += out[1][0][j].x * rv.x - out[1][0][j].y * rv.y;
+            L[idx] = cadd(L[idx], cscale(out[1][0][j], cf));
+          }
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           if (lane == 0) p.leafval[(size_t)b * p.nleaf + node.leaf] = v;
         }

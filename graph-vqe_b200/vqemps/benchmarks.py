@@ -165,12 +165,14 @@ def main(argv=None):
     ap.add_argument("which", choices=["partitions", "gradient", "graphs", "all"])
     ap.add_argument("--reps", type=int, default=None, help="timed repetitions per measurement")
     ap.add_argument("--every", type=int, nargs="+", default=[8, 1], help="gradient checkpoint intervals")
+    ap.add_argument("--plans", nargs="+", default=["auto", "off"], choices=["auto", "off", "on"],
+                    help="gradient plans: split evaluation when it saves work (auto), prefix trie (off)")
     args = ap.parse_args(argv)
     torch.cuda.set_device(0)
     if args.which in ("partitions", "all"):
         bench_partitions(**({"reps": args.reps} if args.reps else {}))
     if args.which in ("gradient", "all"):
-        bench_gradient(every=args.every, **({"reps": args.reps} if args.reps else {}))
+        bench_gradient(every=args.every, plans=args.plans, **({"reps": args.reps} if args.reps else {}))
     if args.which in ("graphs", "all"):
         bench_graphs(**({"reps": args.reps} if args.reps else {}))
 
