@@ -92,7 +92,8 @@ struct EvolveSmem {
   static constexpr int SIG = NORM + 32 * 8;                // 32 sorted singular values
   static constexpr int PERM = SIG + 32 * 8;                // 32 ints
   static constexpr int MISC = PERM + 32 * 4;               // scalars
-  static constexpr int PEND = MISC + 64;                   // n x 4 cplx pending 1q matrices
+  static constexpr int SCHED = MISC + 64;                  // 32 x 16 ints: Jacobi pairs of the gate
+  static constexpr int PEND = SCHED + 32 * 16 * 4;         // n x 4 cplx pending 1q matrices
   static __host__ __device__ int bytes(int n) { return PEND + n * 4 * 16 + (n + 1) * 4 + 16; }
 };
 
@@ -144,15 +145,28 @@ __device__ __noinline__ void apply_2x2_to_site(const cplx *u, cplx *a, int tid, 
 struct EvolveShared {
   cplx *X, *VT, *SA, *SB, *G;
   double *NORM, *SIG;
-  int *PERM, *MISC;
+  int *PERM, *MISC, *SCHED;
 };
+
+// NORM[row] = sum_j |X[row][j]|^2 for rows < mr (even), 16 lanes per row, by
+// the whole CTA (the two 16-lane groups of a warp take rows 2w + 16t and
+// 2w + 1 + 16t, so the width-16 shuffles run on uniform warps).
+__device__ __forceinline__ void jacobi_row_norms(const cplx *X, double *NORM, int mr, int mc, int tid) {
+  const int grp = tid >> 4, lane = tid & 15;
+  for (int row = grp; row < mr; row += EVOLVE_THREADS / 16) {
+    double a = 0.0;
+    for (int j = lane; j < mc; j += 16) a += cabs2(X[row * 32 + j]);
+    for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o, 16);
+    if (lane == 0) NORM[row] = a;
+  }
+}
 
 __device__ __forceinline__ int two_site_update(const EvolveParams &p, const EvolveShared &sh, cplx *sites_b, int s,
                                             int dl, int dc, int dr, cplx *us, cplx *ut, const cplx *gm,
                                             int *bond_next) {
   cplx *X = sh.X, *VT = sh.VT, *SA = sh.SA, *SB = sh.SB, *G = sh.G;
   double *NORM = sh.NORM, *SIG = sh.SIG;
-  int *PERM = sh.PERM, *MISC = sh.MISC;
+  int *PERM = sh.PERM, *MISC = sh.MISC, *SCHED = sh.SCHED;
   const int tid = threadIdx.x;
   const double eps = 2.2204460492503131e-16;
     // ---- two-site gate on (s, s+1) ----
@@ -222,30 +236,35 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
     // ---- one-sided Jacobi on the rows of Theta, round-robin pair ordering ----
     // A pair (p, q) with alpha = |X_p|^2, beta = |X_q|^2, gamma = X_p . X_q^H is
     // rotated by J = c [[1, -w gamma], [w conj(gamma), 1]] with
-    // w = 2 sign(d) / (|d| + sqrt(d^2 + 4 |gamma|^2)), d = beta - alpha,
+    // w = 2 sign(d) / (|d| + r), r = sqrt(d^2 + 4 |gamma|^2), d = beta - alpha,
     // c = 1 / sqrt(1 + w^2 |gamma|^2): the classical Jacobi rotation with the
-    // phase of gamma moved onto row q (V absorbs it). Row norms then move by
-    // -+ w |gamma|^2 and are kept in NORM, recomputed exactly after each sweep.
+    // phase of gamma moved onto row q (V absorbs it). Without a division:
+    // 1 + w^2 |gamma|^2 = 2 r / (|d| + r), so with s = 1 / sqrt(r (|d| + r)),
+    // w c = sign(d) sqrt(2) s, c = (|d| + r) s / sqrt(2) and
+    // w |gamma|^2 = sign(d) 2 |gamma|^2 r s^2. Row norms move by -+ w |gamma|^2
+    // and are kept in NORM, recomputed exactly after each sweep.
     const int pair = tid >> 4, lane = tid & 15;
     const int npairs = mr >> 1;
-    if (tid < mr) {
-      double a = 0.0;
-      for (int j = 0; j < mc; ++j) a += cabs2(X[tid * 32 + j]);
-      NORM[tid] = a;
+    // round-robin pairs of every step of a sweep (row 0 fixed, rows 1 .. mr-1 rotating)
+    for (int e = tid; e < (mr - 1) * 16; e += EVOLVE_THREADS) {
+      const int step = e >> 4, pr_ = e & 15, mm1 = mr - 1;
+      int a = 0, b = 0;
+      if (pr_ < npairs) {
+        if (pr_ == 0) { a = 0; b = 1 + (step % mm1); }
+        else { a = 1 + ((step + pr_) % mm1); b = 1 + ((step + mm1 - pr_) % mm1); }
+        if (a > b) { const int t = a; a = b; b = t; }
+      }
+      SCHED[e] = a | (b << 8);
     }
+    jacobi_row_norms(X, NORM, mr, mc, tid);
     __syncthreads();
     bool converged = false;
     for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
       int rotated = 0;
       for (int step = 0; step < mr - 1; ++step) {
-        int pr = 0, qr = 0;
         const bool active = pair < npairs;
-        if (active) {
-          const int mm1 = mr - 1;
-          if (pair == 0) { pr = 0; qr = 1 + (step % mm1); }
-          else { pr = 1 + ((step + pair) % mm1); qr = 1 + ((step + mm1 - pair) % mm1); }
-          if (pr > qr) { int t = pr; pr = qr; qr = t; }
-        }
+        const int pq = SCHED[step * 16 + pair];
+        const int pr = pq & 255, qr = pq >> 8;
         cplx xp0 = cmake(0, 0), xq0 = cmake(0, 0), xp1 = cmake(0, 0), xq1 = cmake(0, 0);
         const int j0 = lane, j1 = lane + 16;
         if (active) {
@@ -263,38 +282,37 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
         const double g2 = gr * gr + gim * gim;
         if (active && g2 > floor2 && g2 > tol2 * al * be) {
           rotated = 1;
-          const double d = be - al;
-          const double w = copysign(2.0, d) / (fabs(d) + sqrt(d * d + 4.0 * g2));
-          const double c = rsqrt(1.0 + w * w * g2);
-          const cplx wg = cmake(w * gr, w * gim);             // w gamma
-          const cplx wgc = cconj(wg);                         // w conj(gamma)
+          const double d = be - al, ad = fabs(d);
+          const double r = sqrt(d * d + 4.0 * g2);
+          const double sr = rsqrt(r * (ad + r));
+          const double wc = copysign(1.4142135623730951 * sr, d);   // w c
+          const double c = (ad + r) * sr * 0.7071067811865476;
+          const double wg2 = copysign(2.0 * g2 * r * sr * sr, d);    // w |gamma|^2
+          const cplx wg = cmake(wc * gr, wc * gim);           // w c gamma
+          const cplx wgc = cconj(wg);                         // w c conj(gamma)
           if (j0 < mc) {
-            X[pr * 32 + j0] = cscale(csub(xp0, cmul(wg, xq0)), c);
-            X[qr * 32 + j0] = cscale(cadd(cmul(wgc, xp0), xq0), c);
+            X[pr * 32 + j0] = csub(cscale(xp0, c), cmul(wg, xq0));
+            X[qr * 32 + j0] = cadd(cmul(wgc, xp0), cscale(xq0, c));
           }
           if (j1 < mc) {
-            X[pr * 32 + j1] = cscale(csub(xp1, cmul(wg, xq1)), c);
-            X[qr * 32 + j1] = cscale(cadd(cmul(wgc, xp1), xq1), c);
+            X[pr * 32 + j1] = csub(cscale(xp1, c), cmul(wg, xq1));
+            X[qr * 32 + j1] = cadd(cmul(wgc, xp1), cscale(xq1, c));
           }
-          // V <- V J^H: V_p' = c (V_p - w conj(gamma) V_q), V_q' = c (w gamma V_p + V_q)
+          // V <- V J^H: V_p' = c V_p - w c conj(gamma) V_q, V_q' = w c gamma V_p + c V_q
           for (int i = lane; i < mr; i += 16) {
             const cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
-            VT[pr * 32 + i] = cscale(csub(vp, cmul(wgc, vq)), c);
-            VT[qr * 32 + i] = cscale(cadd(cmul(wg, vp), vq), c);
+            VT[pr * 32 + i] = csub(cscale(vp, c), cmul(wgc, vq));
+            VT[qr * 32 + i] = cadd(cmul(wg, vp), cscale(vq, c));
           }
           if (lane == 0) {
-            NORM[pr] = al - w * g2;
-            NORM[qr] = be + w * g2;
+            NORM[pr] = al - wg2;
+            NORM[qr] = be + wg2;
           }
         }
         __syncthreads();
       }
       converged = !__syncthreads_or(rotated);
-      if (tid < mr) {
-        double a = 0.0;
-        for (int j = 0; j < mc; ++j) a += cabs2(X[tid * 32 + j]);
-        NORM[tid] = a;
-      }
+      jacobi_row_norms(X, NORM, mr, mc, tid);
       __syncthreads();
     }
     // ---- singular values = row norms, sorted descending (stable in row index) ----
@@ -399,7 +417,7 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
     return ST_OK;
 }
 
-__global__ void __launch_bounds__(EVOLVE_THREADS)
+__global__ void __launch_bounds__(EVOLVE_THREADS, 3)
 evolve_kernel(EvolveParams p) {
   extern __shared__ __align__(16) unsigned char smem[];
   cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
@@ -411,6 +429,7 @@ evolve_kernel(EvolveParams p) {
   double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
   int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
   int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
+  int *SCHED = reinterpret_cast<int *>(smem + EvolveSmem::SCHED);
   cplx *PEND = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);
   int *BOND = reinterpret_cast<int *>(smem + EvolveSmem::PEND + p.n * 4 * 16);
 
@@ -451,7 +470,7 @@ evolve_kernel(EvolveParams p) {
       continue;
     }
     const int s = g.site;
-    const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC};
+    const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC, SCHED};
     if (two_site_update(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4, PEND + (s + 1) * 4,
                         p.mats + g.mat, BOND + s + 1) != ST_OK)
       break;
@@ -500,6 +519,7 @@ evolve_pair_kernel(EvolveParams p) {
   double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
   int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
   int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
+  int *SCHED = reinterpret_cast<int *>(smem + EvolveSmem::SCHED);
   cplx *U = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);     // 8 entries: U_s, U_{s+1}
 
   const int tid = threadIdx.x;
@@ -527,7 +547,7 @@ evolve_pair_kernel(EvolveParams p) {
 
   const int t0 = p.step_off ? p.step_off[part] : 0;
   const int t1 = p.step_off ? p.step_off[part + 1] : p.nsteps;
-  const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC};
+  const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC, SCHED};
   for (int t = t0; t < t1; ++t) {
     const int gi = p.sched[2 * t + rank];
     // the other CTA may be writing the status of this step: one vote per CTA
