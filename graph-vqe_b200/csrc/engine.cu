@@ -832,7 +832,8 @@ static int ensure_state_ws(vqemps_ctx *ctx, int B) {
 // B200 at 40 qubits: 1.3x faster at B <= 128, slower at B = 256), so by default
 // they run while B is at most the SM count.
 static bool use_pair_chain(const vqemps_ctx *ctx, int B) {
-  return ctx->evolve_pair > 0 || (ctx->evolve_pair < 0 && B <= ctx->sm_count);
+  // two 128-thread CTAs per state: up to 2 x SM count states stay resident at once
+  return ctx->evolve_pair > 0 || (ctx->evolve_pair < 0 && B <= 2 * ctx->sm_count);
 }
 
 static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaStream_t st) {
@@ -857,7 +858,7 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
     ep.gate_q = ctx->d_gate_q;
     ep.qlist = ctx->d_qlist;
     ep.tail_off = ctx->d_tail_off;
-    evolve_pair_kernel<<<2 * B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+    evolve_pair_kernel<<<2 * B, PAIR_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
   } else {
     evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
   }

@@ -78,7 +78,8 @@ struct EvolveParams {
   const int32_t *part_tail_off;
 };
 
-constexpr int EVOLVE_THREADS = 256;
+constexpr int EVOLVE_THREADS = 256;   // one-CTA gate chain
+constexpr int PAIR_THREADS = 128;     // each CTA of the two-CTA gate chain
 constexpr int JACOBI_MAX_SWEEPS = 40;
 
 // Dynamic shared memory layout (bytes).
@@ -149,11 +150,13 @@ struct EvolveShared {
 };
 
 // NORM[row] = sum_j |X[row][j]|^2 for rows < mr (even), 16 lanes per row, by
-// the whole CTA (the two 16-lane groups of a warp take rows 2w + 16t and
-// 2w + 1 + 16t, so the width-16 shuffles run on uniform warps).
+// the whole CTA of NT threads (the two 16-lane groups of a warp take rows
+// 2w + (NT/16) t and 2w + 1 + (NT/16) t, so the width-16 shuffles run on uniform
+// warps). The sum of a row does not depend on NT.
+template <int NT>
 __device__ __forceinline__ void jacobi_row_norms(const cplx *X, double *NORM, int mr, int mc, int tid) {
   const int grp = tid >> 4, lane = tid & 15;
-  for (int row = grp; row < mr; row += EVOLVE_THREADS / 16) {
+  for (int row = grp; row < mr; row += NT / 16) {
     double a = 0.0;
     for (int j = lane; j < mc; j += 16) a += cabs2(X[row * 32 + j]);
     for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o, 16);
@@ -161,6 +164,7 @@ __device__ __forceinline__ void jacobi_row_norms(const cplx *X, double *NORM, in
   }
 }
 
+template <int NT>
 __device__ __forceinline__ int two_site_update(const EvolveParams &p, const EvolveShared &sh, cplx *sites_b, int s,
                                             int dl, int dc, int dr, cplx *us, cplx *ut, const cplx *gm,
                                             int *bond_next) {
@@ -178,7 +182,7 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
     {
       const cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       const cplx *gb = ga + SITE_ELEMS;
-      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) { SA[e] = __ldcg(ga + e); SB[e] = __ldcg(gb + e); }
+      for (int e = tid; e < SITE_ELEMS; e += NT) { SA[e] = __ldcg(ga + e); SB[e] = __ldcg(gb + e); }
       if (tid < 16) {
         // G' = G (U_s (x) U_{s+1}); G'[IJ, ij] = sum_{i'j'} G[IJ, i'j'] U_s[i', i] U_{s+1}[j', j]
         const int row = tid >> 2, col = tid & 3;
@@ -196,9 +200,8 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       ut[tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
     }
     // Theta[(l*2+I), (J*dr+r)] = sum_ij G'[(I*2+J)*4+(i*2+j)] sum_c A[l,i,c] B[c,j,r]  (k_buildM)
-    double fro = 0.0;
-    if (tid < dl * dr) {
-      const int l = tid / dr, r = tid % dr;
+    for (int lr = tid; lr < dl * dr; lr += NT) {
+      const int l = lr / dr, r = lr % dr;
       cplx t00 = cmake(0, 0), t01 = cmake(0, 0), t10 = cmake(0, 0), t11 = cmake(0, 0);
       for (int c = 0; c < dc; ++c) {
         cplx a0 = SA[(l * 2 + 0) * CHI + c], a1 = SA[(l * 2 + 1) * CHI + c];
@@ -213,18 +216,18 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
         const int I = IJ >> 1, J = IJ & 1;
         if (tall) X[(J * dr + r) * 32 + (l * 2 + I)] = v;
         else X[(l * 2 + I) * 32 + (J * dr + r)] = v;
-        fro += cabs2(v);
       }
     }
     // V = identity (stored transposed: VT[col][row])
-    for (int e = tid; e < 32 * 32; e += EVOLVE_THREADS)
+    for (int e = tid; e < 32 * 32; e += NT)
       VT[e] = cmake((e >> 5) == (e & 31) ? 1.0 : 0.0, 0.0);
-    // ||Theta||_F^2 by block reduction
-    for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
-    if ((tid & 31) == 0) NORM[tid >> 5] = fro;
+    __syncthreads();
+    // row norms, then ||Theta||_F^2 as their sum in row order (the same bits
+    // for every thread count)
+    jacobi_row_norms<NT>(X, NORM, mr, mc, tid);
     __syncthreads();
     double total = 0.0;
-    for (int w = 0; w < EVOLVE_THREADS / 32; ++w) total += NORM[w];
+    for (int w = 0; w < mr; ++w) total += NORM[w];
     // Rows below eps * ||Theta||_F are numerically null: pairs whose coupling
     // |gamma| is below eps^2 ||Theta||_F^2 are left alone, which keeps a
     // rank-deficient Theta from rotating rounding noise forever.
@@ -243,10 +246,10 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
     // w c = sign(d) sqrt(2) s, c = (|d| + r) s / sqrt(2) and
     // w |gamma|^2 = sign(d) 2 |gamma|^2 r s^2. Row norms move by -+ w |gamma|^2
     // and are kept in NORM, recomputed exactly after each sweep.
-    const int pair = tid >> 4, lane = tid & 15;
-    const int npairs = mr >> 1;
+    const int grp = tid >> 4, lane = tid & 15;
+    const int npairs = mr >> 1, plim = (npairs + 1) & ~1;
     // round-robin pairs of every step of a sweep (row 0 fixed, rows 1 .. mr-1 rotating)
-    for (int e = tid; e < (mr - 1) * 16; e += EVOLVE_THREADS) {
+    for (int e = tid; e < (mr - 1) * 16; e += NT) {
       const int step = e >> 4, pr_ = e & 15, mm1 = mr - 1;
       int a = 0, b = 0;
       if (pr_ < npairs) {
@@ -256,63 +259,68 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       }
       SCHED[e] = a | (b << 8);
     }
-    jacobi_row_norms(X, NORM, mr, mc, tid);
     __syncthreads();
     bool converged = false;
     for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
       int rotated = 0;
       for (int step = 0; step < mr - 1; ++step) {
-        const bool active = pair < npairs;
-        const int pq = SCHED[step * 16 + pair];
-        const int pr = pq & 255, qr = pq >> 8;
-        cplx xp0 = cmake(0, 0), xq0 = cmake(0, 0), xp1 = cmake(0, 0), xq1 = cmake(0, 0);
-        const int j0 = lane, j1 = lane + 16;
-        if (active) {
-          if (j0 < mc) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
-          if (j1 < mc) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
-        }
-        // gamma = sum_j X[p,j] conj(X[q,j])
-        double gr = xp0.x * xq0.x + xp0.y * xq0.y + xp1.x * xq1.x + xp1.y * xq1.y;
-        double gim = xp0.y * xq0.x - xp0.x * xq0.y + xp1.y * xq1.x - xp1.x * xq1.y;
-        for (int o = 8; o > 0; o >>= 1) {
-          gr += __shfl_xor_sync(0xffffffffu, gr, o, 16);
-          gim += __shfl_xor_sync(0xffffffffu, gim, o, 16);
-        }
-        const double al = active ? NORM[pr] : 0.0, be = active ? NORM[qr] : 0.0;
-        const double g2 = gr * gr + gim * gim;
-        if (active && g2 > floor2 && g2 > tol2 * al * be) {
-          rotated = 1;
-          const double d = be - al, ad = fabs(d);
-          const double r = sqrt(d * d + 4.0 * g2);
-          const double sr = rsqrt(r * (ad + r));
-          const double wc = copysign(1.4142135623730951 * sr, d);   // w c
-          const double c = (ad + r) * sr * 0.7071067811865476;
-          const double wg2 = copysign(2.0 * g2 * r * sr * sr, d);    // w |gamma|^2
-          const cplx wg = cmake(wc * gr, wc * gim);           // w c gamma
-          const cplx wgc = cconj(wg);                         // w c conj(gamma)
-          if (j0 < mc) {
-            X[pr * 32 + j0] = csub(cscale(xp0, c), cmul(wg, xq0));
-            X[qr * 32 + j0] = cadd(cmul(wgc, xp0), cscale(xq0, c));
+        // pairs grp, grp + NT/16, ... of the step (one pass when NT = 256); the
+        // pairs of a step touch disjoint rows, so their order does not matter.
+        // The bound is even, so both 16-lane groups of a warp take the same
+        // passes (the shuffles below need the whole warp).
+        for (int pair = grp; pair < plim; pair += NT / 16) {
+          const bool active = pair < npairs;
+          const int pq = SCHED[step * 16 + pair];
+          const int pr = pq & 255, qr = pq >> 8;
+          cplx xp0 = cmake(0, 0), xq0 = cmake(0, 0), xp1 = cmake(0, 0), xq1 = cmake(0, 0);
+          const int j0 = lane, j1 = lane + 16;
+          if (active) {
+            if (j0 < mc) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
+            if (j1 < mc) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
           }
-          if (j1 < mc) {
-            X[pr * 32 + j1] = csub(cscale(xp1, c), cmul(wg, xq1));
-            X[qr * 32 + j1] = cadd(cmul(wgc, xp1), cscale(xq1, c));
+          // gamma = sum_j X[p,j] conj(X[q,j])
+          double gr = xp0.x * xq0.x + xp0.y * xq0.y + xp1.x * xq1.x + xp1.y * xq1.y;
+          double gim = xp0.y * xq0.x - xp0.x * xq0.y + xp1.y * xq1.x - xp1.x * xq1.y;
+          for (int o = 8; o > 0; o >>= 1) {
+            gr += __shfl_xor_sync(0xffffffffu, gr, o, 16);
+            gim += __shfl_xor_sync(0xffffffffu, gim, o, 16);
           }
-          // V <- V J^H: V_p' = c V_p - w c conj(gamma) V_q, V_q' = w c gamma V_p + c V_q
-          for (int i = lane; i < mr; i += 16) {
-            const cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
-            VT[pr * 32 + i] = csub(cscale(vp, c), cmul(wgc, vq));
-            VT[qr * 32 + i] = cadd(cmul(wg, vp), cscale(vq, c));
-          }
-          if (lane == 0) {
-            NORM[pr] = al - wg2;
-            NORM[qr] = be + wg2;
+          const double al = active ? NORM[pr] : 0.0, be = active ? NORM[qr] : 0.0;
+          const double g2 = gr * gr + gim * gim;
+          if (active && g2 > floor2 && g2 > tol2 * al * be) {
+            rotated = 1;
+            const double d = be - al, ad = fabs(d);
+            const double r = sqrt(d * d + 4.0 * g2);
+            const double sr = rsqrt(r * (ad + r));
+            const double wc = copysign(1.4142135623730951 * sr, d);   // w c
+            const double c = (ad + r) * sr * 0.7071067811865476;
+            const double wg2 = copysign(2.0 * g2 * r * sr * sr, d);    // w |gamma|^2
+            const cplx wg = cmake(wc * gr, wc * gim);           // w c gamma
+            const cplx wgc = cconj(wg);                         // w c conj(gamma)
+            if (j0 < mc) {
+              X[pr * 32 + j0] = csub(cscale(xp0, c), cmul(wg, xq0));
+              X[qr * 32 + j0] = cadd(cmul(wgc, xp0), cscale(xq0, c));
+            }
+            if (j1 < mc) {
+              X[pr * 32 + j1] = csub(cscale(xp1, c), cmul(wg, xq1));
+              X[qr * 32 + j1] = cadd(cmul(wgc, xp1), cscale(xq1, c));
+            }
+            // V <- V J^H: V_p' = c V_p - w c conj(gamma) V_q, V_q' = w c gamma V_p + c V_q
+            for (int i = lane; i < mr; i += 16) {
+              const cplx vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
+              VT[pr * 32 + i] = csub(cscale(vp, c), cmul(wgc, vq));
+              VT[qr * 32 + i] = cadd(cmul(wg, vp), cscale(vq, c));
+            }
+            if (lane == 0) {
+              NORM[pr] = al - wg2;
+              NORM[qr] = be + wg2;
+            }
           }
         }
         __syncthreads();
       }
       converged = !__syncthreads_or(rotated);
-      jacobi_row_norms(X, NORM, mr, mc, tid);
+      jacobi_row_norms<NT>(X, NORM, mr, mc, tid);
       __syncthreads();
     }
     // ---- singular values = row norms, sorted descending (stable in row index) ----
@@ -356,7 +364,7 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       // Theta = V X: left = V[:, perm[:k]], right = X[perm[:k], :]
       cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       cplx *gb = ga + SITE_ELEMS;
-      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) {
+      for (int e = tid; e < SITE_ELEMS; e += NT) {
         const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
         ga[e] = (l < dl && c < k) ? VT[PERM[c] * 32 + (l * 2 + I)] : cmake(0, 0);
         const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
@@ -371,7 +379,7 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       // orthonormal completion does in the reference.
       cplx *UC = SA;                                   // k x m, UC[c * 32 + row]
       const double tiny = 64.0 * eps * mr * SIG[0];
-      for (int e = tid; e < k * 32; e += EVOLVE_THREADS) {
+      for (int e = tid; e < k * 32; e += NT) {
         const int c = e >> 5, row = e & 31;
         UC[e] = (row < m && SIG[c] > tiny) ? cscale(X[PERM[c] * 32 + row], 1.0 / SIG[c]) : cmake(0, 0);
       }
@@ -405,7 +413,7 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       __syncthreads();
       cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
       cplx *gb = ga + SITE_ELEMS;
-      for (int e = tid; e < SITE_ELEMS; e += EVOLVE_THREADS) {
+      for (int e = tid; e < SITE_ELEMS; e += NT) {
         const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
         ga[e] = (l < dl && c < k) ? UC[c * 32 + (l * 2 + I)] : cmake(0, 0);
         const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
@@ -471,7 +479,7 @@ evolve_kernel(EvolveParams p) {
     }
     const int s = g.site;
     const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC, SCHED};
-    if (two_site_update(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4, PEND + (s + 1) * 4,
+    if (two_site_update<EVOLVE_THREADS>(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4, PEND + (s + 1) * 4,
                         p.mats + g.mat, BOND + s + 1) != ST_OK)
       break;
   }
@@ -505,7 +513,7 @@ __device__ __forceinline__ void pending_product(const EvolveParams &p, const dou
 // in global memory (read past L1 with ld.global.cg, since the other CTA writes
 // them). Both CTAs take every step, whatever the status, so the barrier counts
 // always match; after a failure the remaining gates are skipped.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(EVOLVE_THREADS)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
 evolve_pair_kernel(EvolveParams p) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
@@ -533,14 +541,14 @@ evolve_pair_kernel(EvolveParams p) {
   volatile int32_t *status_b = p.status + b;
 
   // |init>^n product state and unit bonds, split between the two CTAs
-  for (int e = tid + rank * EVOLVE_THREADS; e < n * SITE_ELEMS; e += 2 * EVOLVE_THREADS) {
+  for (int e = tid + rank * PAIR_THREADS; e < n * SITE_ELEMS; e += 2 * PAIR_THREADS) {
     const int el = e % SITE_ELEMS;
     cplx v = cmake(0, 0);
     if (el == 0) v = p.init0;
     else if (el == CHI) v = p.init1;
     sites_b[e] = v;
   }
-  for (int x = tid + rank * EVOLVE_THREADS; x <= n; x += 2 * EVOLVE_THREADS) bonds_b[x] = 1;
+  for (int x = tid + rank * PAIR_THREADS; x <= n; x += 2 * PAIR_THREADS) bonds_b[x] = 1;
   if (rank == 0 && tid == 0) *status_b = ST_OK;
   __threadfence();
   cluster.sync();
@@ -561,7 +569,8 @@ evolve_pair_kernel(EvolveParams p) {
       __syncthreads();
       const int s = g.site;
       const int dl = __ldcg(bonds_b + s), dc = __ldcg(bonds_b + s + 1), dr = __ldcg(bonds_b + s + 2);
-      const int st = two_site_update(p, sh, sites_b, s, dl, dc, dr, U, U + 4, p.mats + g.mat, bonds_b + s + 1);
+      const int st = two_site_update<PAIR_THREADS>(p, sh, sites_b, s, dl, dc, dr, U, U + 4, p.mats + g.mat,
+                                                   bonds_b + s + 1);
       if (st != ST_OK && tid == 0) *status_b = st;
     }
     __threadfence();
@@ -574,7 +583,7 @@ evolve_pair_kernel(EvolveParams p) {
       __syncthreads();
       if (tid == 0) pending_product(p, theta_b, p.tail_off[base + x], p.tail_off[base + x + 1], U);
       __syncthreads();
-      apply_2x2_to_site(U, sites_b + (size_t)x * SITE_ELEMS, tid, EVOLVE_THREADS);
+      apply_2x2_to_site(U, sites_b + (size_t)x * SITE_ELEMS, tid, PAIR_THREADS);
     }
   }
 }

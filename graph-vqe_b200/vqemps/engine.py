@@ -222,7 +222,7 @@ class Engine:
 
     def set_evolve_mode(self, mode: str):
         """Gate chain: 'pair' (two-CTA clusters on a schedule), 'chain' (one CTA, program
-        order) or 'auto' (pair while the batch has at most one state per SM; default)."""
+        order) or 'auto' (pair while the batch has at most two states per SM; default)."""
         check(self.ctx, self.lib.vqemps_set_evolve_mode(self.ctx, {"chain": 0, "pair": 1, "auto": -1}[mode]),
               "set_evolve_mode")
 

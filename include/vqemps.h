@@ -214,8 +214,8 @@ int vqemps_set_split_mode(vqemps_ctx *ctx, int mode);
  * simulator_mps_dist.cu:1392-1406): 1 runs each state on a cluster of two CTAs
  * that apply two-site gates on disjoint site pairs concurrently, on an
  * as-soon-as-possible schedule built with the circuit; 0 runs one CTA per state
- * in program order; -1 (default) uses 1 while the batch has at most as many
- * states as the GPU has SMs, else 0. All give the same states bit for bit. */
+ * in program order; -1 (default) uses 1 while the batch has at most twice as
+ * many states as the GPU has SMs, else 0. All give the same states bit for bit. */
 int vqemps_set_evolve_mode(vqemps_ctx *ctx, int mode);
 
 /* Copy the site tensors of state b of the last batched call to the host:

@@ -142,5 +142,5 @@ def test_autograd_function_backward(api):
     (e * w).sum().backward()
     for b in range(3):
         eref, gref = O.reverse_value_gradient(spec, words, coeffs, th.detach().numpy()[b])
-        assert abs(float(e[b]) - eref) < 1e-10
+        assert abs(float(e[b].detach()) - eref) < 1e-10
         np.testing.assert_allclose(th.grad[b].numpy(), w[b].item() * gref, atol=1e-10)
