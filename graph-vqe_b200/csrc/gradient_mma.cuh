@@ -295,12 +295,9 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    mma_panel_EA(E, A, S, g, t);
-    __syncwarp();
-    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
-    cp_async_commit();
     int idx_child[4] = {-1, -1, -1, -1};
     for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
+    // Y_o = sum over classes of A_src(o) D_src(o)
     double yr[2][4][2], yi[2][4][2];
 #pragma unroll
     for (int rt = 0; rt < 2; ++rt)
@@ -340,15 +337,12 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
 #pragma unroll
       for (int ks = 0; ks < 4; ++ks) {
         // output column tile ct covers panel half o = ct >> 1; operand source src(o)
-        cplx sf[2][2], af[2][2], df[4];
+        cplx af[2][2], df[4];
 #pragma unroll
         for (int o = 0; o < 2; ++o) {
           const int src = cls == 0 ? o : 1 - o;
 #pragma unroll
-          for (int rt = 0; rt < 2; ++rt) {
-            sf[o][rt] = S[(src * CHI + rt * 8 + g) * MMA_S_STRIDE + ks * 4 + t];
-            af[o][rt] = A[(rt * 8 + g) * MMA_A_STRIDE + src * CHI + ks * 4 + t];
-          }
+          for (int rt = 0; rt < 2; ++rt) af[o][rt] = A[(rt * 8 + g) * MMA_A_STRIDE + src * CHI + ks * 4 + t];
         }
 #pragma unroll
         for (int ct = 0; ct < 4; ++ct) {
@@ -359,11 +353,7 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
           for (int ct = 0; ct < 4; ++ct) {
-            const cplx x = sf[ct >> 1][rt], a = af[ct >> 1][rt], d = df[ct];
-            dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
-            dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
-            dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
-            dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
+            const cplx a = af[ct >> 1][rt], d = df[ct];
             dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
             dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
             dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
@@ -371,19 +361,41 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
           }
       }
     }
-    if (p.s > 0) {
-      // Y panel into the S region (S is dead), then Ebar_parent = sum_i Y_i A_i^H
-      __syncwarp();
+    // Y panel into the S region: Y_i[row][c] at S[(i * CHI + row) * MMA_S_STRIDE + c]
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int col = ct * 8 + 2 * t + j;
+          S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(yr[rt][ct][j], yi[rt][ct][j]);
+        }
+    __syncwarp();
+    // site cotangent: Abar_o += E Y_o (= S_src D_src summed over the classes, with S = E A)
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      cplx ef[2], yf[4];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * MMA_E_STRIDE + ks * 4 + t];
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) yf[ct] = S[((ct >> 1) * CHI + ks * 4 + t) * MMA_S_STRIDE + (ct & 1) * 8 + g];
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-        for (int ct = 0; ct < 4; ++ct)
-#pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            const int col = ct * 8 + 2 * t + j;
-            S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(yr[rt][ct][j], yi[rt][ct][j]);
-          }
-      __syncwarp();
+        for (int ct = 0; ct < 4; ++ct) {
+          const cplx x = ef[rt], d = yf[ct];
+          dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
+          dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
+          dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
+          dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
+        }
+    }
+    __syncwarp();   // E is consumed: prefetch the next parent
+    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
+    cp_async_commit();
+    if (p.s > 0) {
+      // parent cotangent Ebar = sum_i Y_i A_i^H
       double orr[2][2][2], oi[2][2][2];
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
