@@ -395,12 +395,16 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
     if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
     cp_async_commit();
     if (p.s > 0) {
-      // parent cotangent Ebar = sum_i Y_i A_i^H
+      // parent cotangent Ebar = sum_i Y_i A_i^H. Cotangents of Hermitian
+      // environments are Hermitian: the tiles (0,0), (0,1), (1,1) are formed and
+      // (1,0) is stored as the conjugate transpose of (0,1).
       double orr[2][2][2], oi[2][2][2];
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-        for (int ct = 0; ct < 2; ++ct) { orr[rt][ct][0] = orr[rt][ct][1] = 0.0; oi[rt][ct][0] = oi[rt][ct][1] = 0.0; }
+        for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) orr[rt][ct][j] = oi[rt][ct][j] = 0.0;
 #pragma unroll
       for (int ks = 0; ks < 8; ++ks) {
         const int kk = ks * 4 + t;            // (i, k) = (kk >> 4, kk & 15)
@@ -413,6 +417,7 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
         for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
           for (int ct = 0; ct < 2; ++ct) {
+            if (rt == 1 && ct == 0) continue;
             // Y conj(A): re = Yr Ar + Yi Ai, im = Yi Ar - Yr Ai
             dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
             dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
@@ -425,10 +430,12 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-        for (int ct = 0; ct < 2; ++ct)
+        for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
           for (int j = 0; j < 2; ++j)
             dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = cmake(orr[rt][ct][j], oi[rt][ct][j]);
+#pragma unroll
+      for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = cmake(orr[0][1][j], -oi[0][1][j]);
     }
     __syncwarp();   // S / D are rewritten by the next group
   }
@@ -453,5 +460,6 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
     dst[e] = acc;
   }
 }
+
 
 }  // namespace vqemps
