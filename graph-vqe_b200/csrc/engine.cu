@@ -897,13 +897,13 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
       break;
     }
     case LV_MMAPF4: {
-      const int gpw = ng >= 4 * MPF_WARPS ? 4 : 1;
+      const int gpw = ng >= 32 * MPF_WARPS ? 8 : (ng >= 4 * MPF_WARPS ? 4 : 1);
       const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
       level_mma_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
     }
     case LV_MMA3PF4: {
-      const int gpw = ng >= 4 * MPF_WARPS ? 4 : 1;
+      const int gpw = ng >= 32 * MPF_WARPS ? 8 : (ng >= 4 * MPF_WARPS ? 4 : 1);
       const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
       level_mma3_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
