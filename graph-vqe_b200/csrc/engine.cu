@@ -881,7 +881,17 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
 // Level kernel variants: the autotuner times each on the caller's workload.
 enum : int { LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5, LV_COUNT = 6 };
 
-static void launch_level_variant(int variant, const LevelParams &lp, int ng, int B, cudaStream_t st) {
+// Parents per warp of the prefetch DMMA kernels: 8 on wide levels, 4 on
+// middling ones, fewer while the whole batch would give less than two waves of
+// resident CTAs (three per SM), so that small batches keep every SM busy. The
+// values do not depend on it: each parent is computed the same way by any warp.
+static int mpf_parents_per_warp(int ng, int B, int sms) {
+  int gpw = ng >= 32 * MPF_WARPS ? 8 : (ng >= 4 * MPF_WARPS ? 4 : 1);
+  while (gpw > 1 && (long long)((ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw)) * B < 6LL * sms) gpw >>= 1;
+  return gpw;
+}
+
+static void launch_level_variant(int variant, const LevelParams &lp, int ng, int B, int sms, cudaStream_t st) {
   switch (variant) {
     case LV_MMA4:
       level_mma_kernel<4><<<dim3((ng + 3) / 4, B), 4 * 32, sizeof(LevelMmaSmem<4>), st>>>(lp);
@@ -897,13 +907,13 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
       break;
     }
     case LV_MMAPF4: {
-      const int gpw = ng >= 32 * MPF_WARPS ? 8 : (ng >= 4 * MPF_WARPS ? 4 : 1);
+      const int gpw = mpf_parents_per_warp(ng, B, sms);
       const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
       level_mma_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
     }
     case LV_MMA3PF4: {
-      const int gpw = ng >= 32 * MPF_WARPS ? 8 : (ng >= 4 * MPF_WARPS ? 4 : 1);
+      const int gpw = mpf_parents_per_warp(ng, B, sms);
       const int ctas = (ng + MPF_WARPS * gpw - 1) / (MPF_WARPS * gpw);
       level_mma3_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
@@ -942,7 +952,7 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       lp.n = n;
       lp.s = s;
       lp.suffix = 1;
-      launch_level_variant(variant == LV_MMA3PF4 ? LV_MMA3PF4 : LV_MMAPF4, lp, ng, B, st);
+      launch_level_variant(variant == LV_MMA3PF4 ? LV_MMA3PF4 : LV_MMAPF4, lp, ng, B, ctx->sm_count, st);
       CUDA_TRY(ctx, cudaGetLastError());
     }
   }
@@ -964,7 +974,7 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.nleaf_total = nleaf;
     lp.n = n;
     lp.s = s;
-    launch_level_variant(variant, lp, ng, B, st);
+    launch_level_variant(variant, lp, ng, B, ctx->sm_count, st);
     CUDA_TRY(ctx, cudaGetLastError());
   }
   if (split && h.npairs > 0) {
