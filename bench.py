@@ -159,22 +159,38 @@ def measure_fp64_peak(torch, device):
     return best
 
 
-PROFILED = {"dmma_pf": "level_mma_pf_kernel_40q.md", "dmma3_pf": "level_mma3_pf_kernel_40q.md"}
-
-
 def profiled_traffic(variant):
-    """DRAM bytes per evaluation of all trie levels, from the committed ncu summary
-    of the same kernel (profiles/<kernel>_40q.md: sum of dram__bytes_read.sum +
-    dram__bytes_write.sum over the 40 level launches of one step at B = 32,
-    divided by 32); None for kernels without such a capture."""
-    if variant not in PROFILED:
-        return None
-    path = ROOT / "profiles" / PROFILED[variant]
+    """DRAM bytes per evaluation of all trie levels of one step, as recorded from
+    an ncu capture of the same kernel in profiles/level_traffic.json (a data file
+    written beside the capture's summary); None for kernels without a capture."""
+    path = ROOT / "profiles" / "level_traffic.json"
     if not path.exists():
         return None
-    import re
-    m = re.search(r"traffic_bytes_per_eval:\s*([0-9.eE+]+)", path.read_text())
-    return float(m.group(1)) if m else None
+    return json.loads(path.read_text()).get("bytes_per_eval", {}).get(variant)
+
+
+GOLDEN = ROOT / "tests" / "golden" / "large_workloads_golden.json"
+
+
+def golden_gate(eng, ham, th, words, coeffs):
+    """Before timing: the timed batch's own outputs must equal the reference's.
+
+    tests/golden/large_workloads_golden.json holds the energies the reference's
+    ReverseMPS computed for four parameter sets of this exact batch (and a digest
+    of the Hamiltonian). The full batch is evaluated once and those four compared
+    at 1e-9 relative; any difference stops the benchmark before a line is printed."""
+    from vqemps import workloads as W
+    g = json.loads(GOLDEN.read_text())["batched_40q"]
+    if W.workload_digest(words, coeffs) != g["digest"]:
+        raise SystemExit("golden gate: the benchmark Hamiltonian differs from the recorded one")
+    e = eng.energy(ham, th).cpu().numpy()
+    worst = 0.0
+    for i, ref in zip(g["indices"], g["energies"]):
+        err = abs(float(e[i]) - ref) / max(1.0, abs(ref))
+        worst = max(worst, err)
+        if not err <= 1e-9:
+            raise SystemExit(f"golden gate: parameter set {i}: {e[i]!r} vs reference {ref!r}")
+    return dict(checked=list(g["indices"]), max_rel_err=worst, tol=1e-9)
 
 
 def cpu_reference_rate(seconds, threads):
@@ -235,9 +251,12 @@ def main():
     th = torch.tensor(thetas, dtype=torch.float64, device=device)
     out = torch.empty(args.batch, dtype=torch.float64, device=device)
     stream = torch.cuda.current_stream(device)
-    # correctness gate before timing (first state against a recorded oracle value is in the tests)
-    e0 = eng.energy(ham, th[:2])
-    assert torch.isfinite(e0).all()
+    # correctness gate before timing: the timed batch against the reference's energies
+    gate = None
+    if args.batch == 256 and rank == 0:
+        gate = golden_gate(eng, ham, th, words, coeffs)
+    else:
+        assert torch.isfinite(eng.energy(ham, th[:2])).all()
 
     fp64_peak = measure_fp64_peak(torch, device)
 
@@ -331,7 +350,8 @@ def main():
                                 l2="working set per step > L2 (env buffers ~4 GB): no flush needed",
                                 plain_evals_per_s=plain_rate, batched_over_plain=value / world / plain_rate,
                                 flops_per_eval=stats["flops"], survey_flops_per_eval=stats["flops_survey"],
-                                trie_node_sites=stats["node_sites"], phases_ms=phases["ms"]),
+                                trie_node_sites=stats["node_sites"], phases_ms=phases["ms"],
+                                golden_gate=gate),
                     roofline=roofline, cpu_baseline=cpu, e2e=e2e,
                     gpu_launches=phases["launches_per_step"] * args.steps,
                     clocks=clock_info)

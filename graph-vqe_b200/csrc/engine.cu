@@ -1000,25 +1000,30 @@ static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
   const int key = batch_bucket(B);
   auto it = h.tuned.find(key);
   if (it != h.tuned.end()) { *variant = it->second; return VQEMPS_OK; }
-  cudaEvent_t e0, e1;
-  CUDA_TRY(ctx, cudaEventCreate(&e0));
-  CUDA_TRY(ctx, cudaEventCreate(&e1));
+  // the two timing events are destroyed on every exit path
+  struct Events {
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ~Events() {
+      if (e0) cudaEventDestroy(e0);
+      if (e1) cudaEventDestroy(e1);
+    }
+  } ev;
+  CUDA_TRY(ctx, cudaEventCreate(&ev.e0));
+  CUDA_TRY(ctx, cudaEventCreate(&ev.e1));
   int best = LV_SIMT4;
   float best_ms = 1e30f;
   for (int v = 0; v < LV_COUNT; ++v) {
     int rc = run_levels(ctx, h, B, st, v);      // warm
     if (rc) return rc;
-    CUDA_TRY(ctx, cudaEventRecord(e0, st));
+    CUDA_TRY(ctx, cudaEventRecord(ev.e0, st));
     rc = run_levels(ctx, h, B, st, v);
     if (rc) return rc;
-    CUDA_TRY(ctx, cudaEventRecord(e1, st));
-    CUDA_TRY(ctx, cudaEventSynchronize(e1));
+    CUDA_TRY(ctx, cudaEventRecord(ev.e1, st));
+    CUDA_TRY(ctx, cudaEventSynchronize(ev.e1));
     float ms = 0.f;
-    CUDA_TRY(ctx, cudaEventElapsedTime(&ms, e0, e1));
+    CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ev.e0, ev.e1));
     if (ms < best_ms) { best_ms = ms; best = v; }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   h.tuned[key] = best;
   *variant = best;
   return VQEMPS_OK;

@@ -22,7 +22,13 @@
 // different streams, or from different threads) race on it and must be
 // serialised by the caller. The first call on each device looks up the array's
 // device address (cudaGetSymbolAddress with that device current); make that
-// first call before any stream capture.
+// first call before any stream capture. The address is remembered together with
+// the CUDA context it belongs to: after a device reset (or any other change of
+// the context current on the device) the next call looks it up again, so it is
+// that call, too, that must come before any stream capture. The call leaves the
+// caller's current device as it found it.
+
+#include <cuda.h>   // the CUcontext type only; the driver function is looked up at run time
 
 #include <mutex>
 
@@ -47,22 +53,62 @@ static_assert(NA_STATUS + 256 <= NOALLOC_SCRATCH_BYTES, "scratch layout exceeds 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 
 std::mutex g_noalloc_mutex;
-unsigned char *g_noalloc_addr[128] = {nullptr};
+struct NoallocAddr {
+  CUcontext context;
+  unsigned char *addr;
+};
+NoallocAddr g_noalloc_addr[128] = {};
 
-// Device address of the scratch array on `device` (which must be current).
+// The CUDA context current on the calling thread (null if the driver cannot be
+// asked). cuCtxGetCurrent is fetched through the runtime, so the library does
+// not link against the driver library and still loads on machines without one.
+CUcontext noalloc_current_context() {
+  typedef CUresult (*GetCurrent)(CUcontext *);
+  static GetCurrent fn = [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (GetCurrent) nullptr;
+    return reinterpret_cast<GetCurrent>(p);
+  }();
+  CUcontext c = nullptr;
+  if (fn == nullptr || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
+
+// Device address of the scratch array on `device` (which must be current), looked
+// up again whenever the current context is not the one of the remembered address.
 int noalloc_scratch(vqemps_ctx *ctx, unsigned char **out) {
   if (ctx->device < 0 || ctx->device >= 128) return fail(ctx, VQEMPS_INVALID, "device index out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (g_noalloc_addr[ctx->device] == nullptr) {
+  NoallocAddr &slot = g_noalloc_addr[ctx->device];
+  const CUcontext current = noalloc_current_context();
+  if (slot.addr == nullptr || current == nullptr || slot.context != current) {
     void *ptr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess)
       return fail(ctx, VQEMPS_CUDA_ERROR, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_noalloc_addr[ctx->device] = static_cast<unsigned char *>(ptr);
+    slot.addr = static_cast<unsigned char *>(ptr);
+    slot.context = current;
   }
-  *out = g_noalloc_addr[ctx->device];
+  *out = slot.addr;
   return VQEMPS_OK;
 }
+
+// Makes `device` current for one call and gives the caller's device back after.
+struct NoallocDeviceScope {
+  int previous = -1;
+  cudaError_t status = cudaSuccess;
+  explicit NoallocDeviceScope(int device) {
+    if (cudaGetDevice(&previous) != cudaSuccess) previous = -1;
+    if (previous != device) status = cudaSetDevice(device);
+  }
+  ~NoallocDeviceScope() {
+    int now = -1;
+    if (previous >= 0 && cudaGetDevice(&now) == cudaSuccess && now != previous) cudaSetDevice(previous);
+  }
+};
 
 }  // namespace
 
@@ -86,7 +132,8 @@ extern "C" int vqemps_energy_noalloc(vqemps_ctx *ctx, int handle, const double *
     return fail(ctx, VQEMPS_INVALID, "vqemps_energy_noalloc: " + std::to_string(h->nleaf) +
                                          " distinct term endings exceed the limit of " +
                                          std::to_string(NOALLOC_MAX_LEAVES));
-  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  NoallocDeviceScope device_scope(ctx->device);
+  CUDA_TRY(ctx, device_scope.status);
   unsigned char *base = nullptr;
   int rc = noalloc_scratch(ctx, &base);
   if (rc) return rc;

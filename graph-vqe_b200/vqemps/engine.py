@@ -324,7 +324,7 @@ class Engine:
         return bits
 
     def sampled_energy(self, ham: Hamiltonian, theta, shots: int, seed: int, rng: str = "splitmix",
-                       mode: str = "shared", per_term: bool = False, stream=None):
+                       mode: str = "shared", per_term: bool = False, stream=None, check_status: bool = True):
         t = self._theta(theta)
         B = t.shape[0]
         e = torch.empty(B, dtype=torch.float64, device=self.device)
@@ -332,7 +332,8 @@ class Engine:
         check(self.ctx, self.lib.vqemps_sampled_energy(self.ctx, ham.handle, _ptr(t), B, shots, seed,
                                                        _lib.RNG[rng], _lib.SHOT_MODES[mode], _ptr(e),
                                                        _ptr(pt), _stream(stream)), "sampled_energy")
-        self.check_status(B, stream)
+        if check_status:
+            self.check_status(B, stream)
         return (e, pt) if per_term else e
 
     # -- partition sets ------------------------------------------------------

@@ -140,17 +140,29 @@ def for_objective(fun, mode):
 class MPSEnergy(torch.autograd.Function):
     """E(theta) for a batch [B, P] of parameter sets; backward uses the adjoint kernels.
 
-    ``MPSEnergy.apply(theta, engine, ham)`` returns the B energies. The forward
-    pass runs the adjoint sweep once and keeps dE/dtheta for the backward pass.
+    ``MPSEnergy.apply(theta, engine, ham)`` returns the B energies. When autograd
+    will need dE/dtheta (grad mode on and ``theta`` requiring grad) the forward
+    pass runs the adjoint sweep once and keeps the gradient for the backward
+    pass; otherwise (under ``torch.no_grad()``, or for a ``theta`` that needs no
+    gradient) it runs the energy-only path, about a third of the cost.
     """
 
+    @classmethod
+    def apply(cls, theta, engine, ham):
+        # grad mode is always off inside forward(), so it is read here
+        need = bool(torch.is_grad_enabled() and getattr(theta, "requires_grad", False))
+        return super().apply(theta, engine, ham, need)
+
     @staticmethod
-    def forward(ctx, theta, engine, ham):
+    def forward(ctx, theta, engine, ham, need_grad):
         th = theta.detach().to(device=engine.device, dtype=torch.float64).contiguous()
         if th.dim() == 1:
             th = th.unsqueeze(0)
-        e, g = engine.energy_grad(ham, th)
-        ctx.save_for_backward(g)
+        if need_grad:
+            e, g = engine.energy_grad(ham, th)
+            ctx.save_for_backward(g)
+        else:
+            e = engine.energy(ham, th)
         ctx.squeeze = theta.dim() == 1
         out = e.to(theta.device)
         return out[0] if ctx.squeeze else out
@@ -160,8 +172,8 @@ class MPSEnergy(torch.autograd.Function):
         (g,) = ctx.saved_tensors
         go = grad_out.to(g.device, torch.float64)
         if ctx.squeeze:
-            return (go * g[0]).to(grad_out.device), None, None
-        return (go[:, None] * g).to(grad_out.device), None, None
+            return (go * g[0]).to(grad_out.device), None, None, None
+        return (go[:, None] * g).to(grad_out.device), None, None, None
 
 
 def mps_energy(theta, engine, ham):

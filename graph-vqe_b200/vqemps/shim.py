@@ -23,6 +23,7 @@ import threading
 from concurrent.futures import Future
 
 import numpy as np
+import torch
 
 from .engine import Engine, counts as _counts
 
@@ -341,27 +342,74 @@ def _next_seed():
     return s
 
 
-def observe(kernel, hamiltonian, *args, shots_count=-1, qpu_id=0, noise_model=None, **_):
-    if noise_model is not None:
-        raise RuntimeError("noise models are not supported by the MPS engine")
+class AsyncObserveResult:
+    """An observe call whose kernels are queued on the engine's stream.
+
+    ``get()`` waits for them, checks the state's status and returns the
+    ObserveResult. The engine keeps one status word per state, which the next
+    call on the same engine overwrites, so submitting another call on that
+    engine first finishes this one (its result or error is kept for ``get()``);
+    calls on other kernels' engines overlap freely."""
+
+    def __init__(self, eng, ws, e, pt):
+        self._eng, self._ws, self._e, self._pt = eng, ws, e, pt
+        self._event = torch.cuda.Event()
+        self._event.record(torch.cuda.current_stream(eng.device))
+        self._future = None
+
+    def done(self):
+        return self._future is not None or self._event.query()
+
+    def _finish(self):
+        if self._future is not None:
+            return
+        f = Future()
+        try:
+            self._event.synchronize()
+            self._eng.check_status(1)
+            f.set_result(ObserveResult(float(self._e[0]), self._ws, self._pt[0].cpu().numpy()))
+        except BaseException as exc:      # kept for get(), as a Future does
+            f.set_exception(exc)
+        self._future = f
+        if _pending.get(id(self._eng)) is self:
+            del _pending[id(self._eng)]
+
+    def get(self):
+        self._finish()
+        return self._future.result()
+
+
+_pending = {}
+
+
+def _submit(kernel, hamiltonian, args, shots_count):
     eng = _runner.engine(kernel)
+    prev = _pending.get(id(eng))
+    if prev is not None:
+        prev._finish()
     h, ws = _runner.ham(kernel, eng, hamiltonian)
     ang = kernel.angles(args)
     if shots_count is None or shots_count < 0:
-        e, pt = eng.energy(h, ang, per_term=True)
+        e, pt = eng.energy(h, ang, per_term=True, check_status=False)
     else:
-        e, pt = eng.sampled_energy(h, ang, int(shots_count), _next_seed(), "splitmix", "plugin", per_term=True)
-    return ObserveResult(float(e[0]), ws, pt[0].cpu().numpy())
+        e, pt = eng.sampled_energy(h, ang, int(shots_count), _next_seed(), "splitmix", "plugin", per_term=True,
+                                   check_status=False)
+    res = AsyncObserveResult(eng, ws, e, pt)
+    _pending[id(eng)] = res
+    return res
 
 
-def observe_async(kernel, hamiltonian, *args, **kw):
-    f = Future()
-    f.set_result(observe(kernel, hamiltonian, *args, **kw))
+def observe(kernel, hamiltonian, *args, shots_count=-1, qpu_id=0, noise_model=None, **_):
+    if noise_model is not None:
+        raise RuntimeError("noise models are not supported by the MPS engine")
+    return _submit(kernel, hamiltonian, args, shots_count).get()
 
-    class _Async:
-        def get(self):
-            return f.result()
-    return _Async()
+
+def observe_async(kernel, hamiltonian, *args, shots_count=-1, qpu_id=0, noise_model=None, **_):
+    """Queue the evaluation and return at once; ``.get()`` waits for it."""
+    if noise_model is not None:
+        raise RuntimeError("noise models are not supported by the MPS engine")
+    return _submit(kernel, hamiltonian, args, shots_count)
 
 
 def sample(kernel, *args, shots_count=1000, **_):

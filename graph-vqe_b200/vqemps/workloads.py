@@ -14,6 +14,8 @@ Words are strings over I/X/Y/Z indexed by qubit. Circuits are spec dicts
 """
 from __future__ import annotations
 
+import hashlib
+
 import numpy as np
 
 from .strategy import ansatz_ops
@@ -40,6 +42,15 @@ def random_hamiltonian(rng: np.random.Generator, n: int, terms: int, wmax: int, 
             sign = 1.0 if rng.random() < 0.5 else -1.0
             coeffs.append(sign * float(rng.uniform(100.0, 1000.0)))
     return words, np.asarray(coeffs, dtype=np.float64)
+
+
+def workload_digest(words, coeffs) -> str:
+    """SHA-256 of a Hamiltonian: the words newline-joined in ASCII, then the
+    coefficients as little-endian FP64. Pins a regenerated workload to recorded
+    values without storing its terms."""
+    h = hashlib.sha256("\n".join(words).encode("ascii"))
+    h.update(np.ascontiguousarray(coeffs, dtype="<f8").tobytes())
+    return h.hexdigest()
 
 
 def plain_12q(seed: int = 0):

@@ -275,7 +275,10 @@ int vqemps_partition_sampled_energy(vqemps_ctx *ctx, int handle, const double *t
  * on one site, <= 16384 distinct term endings (VQEMPS_INVALID beyond them).
  * Calls share that array: calls that overlap on the GPU race and must be
  * serialised by the caller. The first call on a device looks the array up
- * (make it before any stream capture). theta_dev: P doubles; energy_dev: 1
+ * (make it before any stream capture); the address is tied to the CUDA context
+ * current at that call, and after a device reset the next call looks it up
+ * again (it too must come before any capture). The caller's current device is
+ * the same after the call as before it. theta_dev: P doubles; energy_dev: 1
  * double (NaN if the state failed); per_term_dev: T doubles or NULL;
  * status_dev: 1 int32 (vqemps_status of the state) or NULL. */
 int vqemps_energy_noalloc(vqemps_ctx *ctx, int handle, const double *theta_dev, double *energy_dev,

@@ -7,13 +7,24 @@ set of seeded cases to ``reverse_mps_golden.json`` next to this script. The
 reference checkout does not exist where the GPU tests run, so the vectors are
 committed and this script is only rerun by hand.
 
-Usage: python tests/golden/make_golden.py
+Usage: python tests/golden/make_golden.py            (small cases, words inline)
+       python tests/golden/make_golden.py --large    (benchmark-size cases)
+
+``--large`` writes ``large_workloads_golden.json``: the reference's energies for
+four parameter sets of the 40-qubit / 5,000-term / B = 256 benchmark batch
+(``vqemps.workloads.batched_40q(seed=0)``) and energy plus full gradient for two
+parameter sets of the 64-qubit / 20,000-term gradient workload
+(``vqemps.workloads.gradient_64q(seed=0)``). Those Hamiltonians are too large to
+store inline; the file records the generator call and a SHA-256 digest of the
+words and coefficients, which the tests and the benchmark check before they
+compare.
 """
 from __future__ import annotations
 
 import json
 import os
 import sys
+import time
 from pathlib import Path
 
 import numpy as np
@@ -94,5 +105,51 @@ def main():
     print(f"wrote {len(out)} cases")
 
 
+def _check_spec(name, spec, n, pattern):
+    ref = registered_spec(n, 4, ("ry",), pattern)
+    ours = [tuple(o) for o in spec["ops"]]
+    assert ours == [tuple(o) for o in ref["ops"]] and spec["count"] == ref["count"], name
+    return ref
+
+
+def main_large():
+    sys.path.insert(0, str(REPO / "graph-vqe_b200"))
+    from vqemps import workloads as VW  # the generators bench.py and the tests use
+    workload_digest = VW.workload_digest
+    import torch
+    torch.set_num_threads(os.cpu_count() or 1)
+    out = {}
+    # the benchmark batch: 40 qubits, reverse_linear, 5,000 terms, 256 SPSA probes
+    spec, words, coeffs, thetas = VW.batched_40q(seed=0, batch=256)
+    ref = _check_spec("batched_40q", spec, 40, "reverse_linear")
+    idx = [0, 1, 128, 255]
+    cases = []
+    for i in idx:
+        t0 = time.time()
+        c = case(f"batched_40q_{i}", ref, words, coeffs, thetas[i], grad=False)
+        cases.append(c["energy"])
+        print(f"batched_40q[{i}] E = {c['energy']!r} ({time.time() - t0:.1f} s)", flush=True)
+    out["batched_40q"] = dict(call="vqemps.workloads.batched_40q(seed=0, batch=256)", n=40, terms=len(words),
+                              digest=workload_digest(words, coeffs), indices=idx, energies=cases)
+    # the gradient workload: 64 qubits, linear, 20,000 terms, 32 parameter sets
+    spec, words, coeffs, thetas = VW.gradient_64q(seed=0, batch=32)
+    ref = _check_spec("gradient_64q", spec, 64, "linear")
+    idx = [0, 17]
+    es, gs = [], []
+    for i in idx:
+        t0 = time.time()
+        c = case(f"gradient_64q_{i}", ref, words, coeffs, thetas[i], grad=True)
+        es.append(c["energy"])
+        gs.append(c["gradient"])
+        print(f"gradient_64q[{i}] E = {c['energy']!r} ({time.time() - t0:.1f} s)", flush=True)
+    out["gradient_64q"] = dict(call="vqemps.workloads.gradient_64q(seed=0, batch=32)", n=64, terms=len(words),
+                               digest=workload_digest(words, coeffs), indices=idx, energies=es, gradients=gs)
+    (HERE / "large_workloads_golden.json").write_text(json.dumps(out))
+    print("wrote large_workloads_golden.json")
+
+
 if __name__ == "__main__":
-    main()
+    if "--large" in sys.argv:
+        main_large()
+    else:
+        main()

@@ -52,6 +52,30 @@ def test_observe_matches_oracle_and_async(api):
     assert abs(r.expectation(sub) - O.dense_expectations(psi, ["IZZIII"])[0].real) < 1e-10
 
 
+def test_observe_async_overlaps_kernels_and_keeps_each_result(api):
+    """Several observe_async calls are queued before any get(): on two kernels
+    (two engines) and twice on the same kernel, whose second submission first
+    finishes the first one. Each result equals the synchronous observe."""
+    shim, _ = api
+    k1, spec1 = build_ansatz(shim, 6, 2)
+    k2, spec2 = build_ansatz(shim, 8, 3, pattern="reverse_linear")
+    rng = np.random.default_rng(5)
+    x1 = rng.uniform(-np.pi, np.pi, spec1["count"])
+    x2 = rng.uniform(-np.pi, np.pi, spec2["count"])
+    H1 = 0.4 * shim.spin.z(0) - 0.7 * shim.spin.z(1) * shim.spin.z(2) + 0.2 * shim.spin.x(3) * shim.spin.y(5)
+    H2 = 1.3 * shim.spin.z(7) * shim.spin.z(0) - 0.5 * shim.spin.x(4) + 0.25
+    ref1 = shim.observe(k1, H1, *x1).expectation()
+    ref1b = shim.observe(k1, H1, *(-x1)).expectation()
+    ref2 = shim.observe(k2, H2, *x2).expectation()
+    a = shim.observe_async(k1, H1, *x1, qpu_id=0)
+    b = shim.observe_async(k2, H2, *x2, qpu_id=1)
+    c = shim.observe_async(k1, H1, *(-x1), qpu_id=0)
+    assert c.get().expectation() == ref1b
+    assert b.get().expectation() == ref2
+    assert a.get().expectation() == ref1
+    assert a.done() and b.done() and c.done()
+
+
 def test_known_answer_two_qubits_through_the_shim(api):
     shim, _ = api
     kernel, theta = shim.make_kernel(float)

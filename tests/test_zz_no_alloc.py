@@ -5,9 +5,11 @@ simulator plugin inside a runtime that owns the device memory, an operator
 under a fixed memory budget): all of its scratch lives in one static device
 array. This file is collected last so that a run stopping at the first
 failure has already run every other test; it also passes alone in a fresh
-process. The check: through the C ABI, two calls in a row give the energies and
+process. The checks: through the C ABI, two calls in a row give the energies and
 per-term values of the existing batched entry point within the tolerance of the
-other energy tests (1e-9 relative), and sizes beyond the limits are refused.
+other energy tests (1e-9 relative); further calls leave the device's free memory
+unchanged (they allocate nothing); the caller's current device is kept; and
+sizes beyond the limits are refused.
 """
 import ctypes
 
@@ -51,6 +53,40 @@ def test_noalloc_energy_matches_batched_entry_point_on_two_calls(cuda_device):
             assert abs(float(e[0]) - float(ref_e[0])) <= RTOL * max(1.0, abs(float(ref_e[0])))
             np.testing.assert_allclose(pt.cpu().numpy(), ref_pt[0].cpu().numpy(), rtol=0, atol=1e-11)
         eng.close()
+
+
+def test_noalloc_calls_allocate_no_device_memory(cuda_device):
+    """On a fresh engine, after its circuit and Pauli sum are loaded and one warm
+    call (which loads the kernels), more calls leave cudaMemGetInfo's free
+    memory exactly as it was; no batched call runs before, so no workspace of
+    the engine could have been grown by them."""
+    import vqemps
+    from vqemps import _lib
+    lib = _lib.load()
+    spec, words, coeffs, thetas = W.batched_40q(0, batch=4)
+    eng = vqemps.Engine(0, 16)
+    eng.set_spec(spec)
+    ham = eng.set_hamiltonian(words, coeffs)
+    th = torch.tensor(thetas, dtype=torch.float64, device="cuda:0")
+    e = torch.empty(4, dtype=torch.float64, device="cuda:0")
+    st = torch.empty(4, dtype=torch.int32, device="cuda:0")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def call(k):
+        code = lib.vqemps_energy_noalloc(eng.ctx, ham.handle, _p(th[k]), _p(e[k:]), None, _p(st[k:]), stream)
+        assert code == _lib.OK, lib.vqemps_last_error(eng.ctx)
+
+    call(0)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for k in range(1, 4):
+        call(k)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
+    assert (st == 0).all() and torch.isfinite(e).all()
+    assert torch.cuda.current_device() == 0
+    eng.close()
 
 
 def test_noalloc_refuses_sizes_beyond_its_limits(cuda_device):
