@@ -114,6 +114,27 @@ struct PairSched {
   int nsteps = 0;
 };
 
+// Which factor of each two-site gate carries the singular values (a gauge choice,
+// see evolve.cuh): the left one when the next two-site gate that touches either
+// of its sites touches only its right site, else the right one (the reference's
+// packing). Leaves every one-site gate's flags at 0.
+void mark_sigma_side(std::vector<DevGate> &gates) {
+  for (size_t i = 0; i < gates.size(); ++i) {
+    if (gates[i].kind != GATE_TWO) continue;
+    const int s = gates[i].site;
+    int flags = 0;
+    for (size_t j = i + 1; j < gates.size(); ++j) {
+      if (gates[j].kind != GATE_TWO) continue;
+      const int t = gates[j].site;                  // touches t and t + 1
+      const bool left = (t == s || t + 1 == s), right = (t == s + 1 || t + 1 == s + 1);
+      if (!left && !right) continue;
+      flags = (right && !left) ? GATE_SIGMA_LEFT : 0;
+      break;
+    }
+    gates[i].flags = flags;
+  }
+}
+
 PairSched build_pair_schedule(const std::vector<DevGate> &gates, int n) {
   PairSched ps;
   ps.gate_q.assign(4 * std::max<size_t>(gates.size(), 1), 0);
@@ -515,6 +536,7 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
       doubling_ok = false;
     }
   }
+  mark_sigma_side(gates);
   // upload
   cudaFree(ctx->d_gates); ctx->d_gates = nullptr;
   cudaFree(ctx->d_mats); ctx->d_mats = nullptr;
