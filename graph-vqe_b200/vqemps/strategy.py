@@ -34,9 +34,7 @@ import time
 from itertools import combinations
 
 import numpy as np
-from scipy.optimize import minimize
-
-from . import _lib
+from . import _lib, optimize
 from ._lib import EngineError
 
 
@@ -78,10 +76,6 @@ def ansatz_ops(n_active, reps, gates, pattern):
         if layer < reps and n_active > 1:
             ops.extend(("cx", a, b) for a, b in pairs_for_pattern(n_active, pattern))
     return ops, index
-
-
-class EarlyStop(Exception):
-    pass
 
 
 class _RoundBatcher:
@@ -143,29 +137,22 @@ class _RoundBatcher:
 
 
 def minimize_model(params, maxiter, constant, energies, value_grad, *, energy_tol=1.0,
-                   use_gradient_optimizer=True):
-    """One model's optimisation (independent_vqe.py:176-245).
+                   use_gradient_optimizer=True, line_search="scipy"):
+    """One model's optimisation (independent_vqe.py:176-245) through the drivers
+    of :mod:`vqemps.optimize`: L-BFGS-B (ftol 1e-12, gtol 1e-8) or COBYLA (tol
+    1e-8), both stopping once an accepted iterate improves the energy by less
+    than ``energy_tol``.
 
     ``energies(X)`` -> energies of the rows of X; ``value_grad(x)`` -> (E, dE/dx),
-    or None to use the parameter-shift rule through ``energies``."""
+    or None to use the parameter-shift rule through ``energies`` (the 2P shifted
+    points and the centre in one call). ``line_search="batched"`` evaluates the
+    L-BFGS step lengths several per call (:func:`vqemps.optimize.lbfgs_batched`)."""
     params = np.asarray(params, dtype=float).copy()
-    cache = {}
-    grads = {}
-    best = [float("inf"), params.copy()]
-    previous = [None]
-    accepted = [0]
-    reason = ["iteration_limit"]
     history = []
-
-    def record(x, e):
-        cache[np.asarray(x).tobytes()] = e
-        if previous[0] is None:
-            previous[0] = e
-        if e < best[0]:
-            best[:] = [e, np.asarray(x).copy()]
-        history.append(e)
+    accepted = [0]
 
     def evaluate_with_gradient(x):
+        x = np.asarray(x, dtype=float)
         if value_grad is not None:
             e, g = value_grad(x)
         else:
@@ -176,52 +163,38 @@ def minimize_model(params, maxiter, constant, energies, value_grad, *, energy_to
             shifted[1 + P + idx, idx] -= np.pi / 2
             v = energies(shifted)
             e, g = v[0], (v[1:P + 1] - v[P + 1:]) / 2
-        grads[np.asarray(x).tobytes()] = np.asarray(g, dtype=float)
-        return float(e)
+        history.append(float(e))
+        return float(e), np.asarray(g, dtype=float)
 
-    def cost(x):
-        key = np.asarray(x).tobytes()
-        if key in cache:
-            return cache[key]
-        e = evaluate_with_gradient(x) if use_gradient_optimizer else float(energies(x[None, :])[0])
-        record(x, e)
+    def evaluate_batch(X):
+        out = [evaluate_with_gradient(x) for x in np.atleast_2d(X)]
+        return np.array([o[0] for o in out]), np.array([o[1] for o in out])
+
+    def energy_only(x):
+        e = float(energies(np.asarray(x, dtype=float)[None, :])[0])
+        history.append(e)
         return e
 
-    def gradient(x):
-        key = np.asarray(x).tobytes()
-        if key not in grads:
-            evaluate_with_gradient(x)
-        return grads[key]
-
-    def callback(*args, **kwargs):
-        x = np.asarray(kwargs.get("intermediate_result").x if "intermediate_result" in kwargs else args[0])
-        key = x.tobytes()
-        e = cache[key] if key in cache else cost(x)
-        improvement = previous[0] - e
-        previous[0] = e
+    def count(_x):
         accepted[0] += 1
-        cache.clear()
-        cache[key] = e
-        if improvement < energy_tol:
-            reason[0] = "energy_improvement_below_threshold"
-            raise EarlyStop()
 
     started = time.perf_counter()
-    cost(params)
     if maxiter and not constant:
-        try:
-            if use_gradient_optimizer:
-                res = minimize(cost, params, method="L-BFGS-B", jac=gradient, callback=callback,
-                               options=dict(maxiter=maxiter, ftol=1e-12, gtol=1e-8))
-            else:
-                res = minimize(cost, params, method="COBYLA", callback=callback,
-                               options=dict(maxiter=maxiter, tol=1e-8))
-            reason[0] = str(res.message)
-        except EarlyStop:
-            pass
-    elif constant:
-        reason[0] = "constant_local_objective"
-    return dict(energy=float(best[0]), params=best[1], accepted_iterations=accepted[0], stop_reason=reason[0],
+        if use_gradient_optimizer:
+            res = optimize.lbfgs_minimize(evaluate_with_gradient, params, maxiter=maxiter, ftol=1e-12, gtol=1e-8,
+                                          immediate_energy_tol=None, accepted_energy_tol=energy_tol, callback=count,
+                                          line_search=line_search, value_grad_batch=evaluate_batch)
+            energy, best_x = float(res.get("best_energy", res.fun)), np.asarray(res.get("best_x", res.x))
+        else:
+            res = optimize.cobyla_minimize(energy_only, params, maxiter, tol=1e-8, accepted_energy_tol=energy_tol,
+                                           callback=count)
+            energy, best_x = float(res.fun), np.asarray(res.x)
+        reason = str(res.message)
+    else:
+        energy = evaluate_with_gradient(params)[0] if use_gradient_optimizer else energy_only(params)
+        best_x = params.copy()
+        reason = "constant_local_objective" if constant else "iteration_limit"
+    return dict(energy=float(energy), params=best_x, accepted_iterations=accepted[0], stop_reason=reason,
                 duration_s=time.perf_counter() - started, history=history)
 
 

@@ -74,3 +74,58 @@ def test_full_plain_method_run(vq):
     ref = O.reverse_energy(dict(n=n, ops=strat.problem.ops, initial=None, count=strat.num_params),
                            strat.plan.words, strat.plan.coeffs, out["best_params"])
     assert abs(ref - out["best_energy"]) <= 1e-9 * max(1.0, abs(ref))
+
+
+def test_run_equals_reference_strategy_golden(vq):
+    """The whole plain method against a run of the reference's own strategy code
+    (tests/golden/strategy_golden.json: IndependentSubspaceVQE's constructor,
+    _partition, _run_vqe and _minimize_model extracted from the source and run
+    with the oracle's energies): the same blocks, local solve energies and
+    iteration counts, warm start, and best energy. Energies agree to the
+    engine's FP64 rounding (1e-9 relative); the optimizers see values that
+    differ in the last bits, so parameters agree to 1e-6."""
+    import json
+    from pathlib import Path
+    from vqemps import workloads as VW
+    from vqemps.strategy import IndependentPartitionVQE
+    g = json.loads((Path(__file__).parent / "golden" / "strategy_golden.json").read_text())
+    words, coeffs = VW.random_hamiltonian(np.random.default_rng(g["hamiltonian_seed"]), g["n"], g["terms"], g["wmax"])
+    assert VW.workload_digest(words, coeffs) == g["digest"]
+    eng = vq.Engine(0, 16)
+    strat = IndependentPartitionVQE(eng, g["n"], words, coeffs, reps=g["reps"], su2_gates=tuple(g["su2_gates"]),
+                                    entanglement=g["entanglement"], max_block_qubits=g["max_block_qubits"],
+                                    energy_tol=g["energy_tol"], block_maxiter=g["block_maxiter"],
+                                    global_maxiter=g["global_maxiter"], use_gradient_optimizer=g["use_gradient_optimizer"],
+                                    seed=g["seed"])
+    out = strat.run()
+    rel = lambda a, b: abs(a - b) / max(1.0, abs(b))  # noqa: E731
+    assert out["blocks"] == g["blocks"]
+    for r, e, acc, stop in zip(out["local_results"], g["local_energies"], g["local_accepted"], g["local_stop"]):
+        assert rel(r["energy"], e) < 1e-9 and r["accepted_iterations"] == acc and r["stop_reason"] == stop
+    np.testing.assert_allclose(out["warm_start_params"], g["warm_start_params"], atol=1e-6)
+    assert rel(out["warm_start_energy"], g["warm_start_energy"]) < 1e-9
+    assert out["global_result"]["accepted_iterations"] == g["global_accepted"]
+    assert rel(out["global_result"]["energy"], g["global_energy"]) < 1e-9
+    assert rel(out["best_energy"], g["best_energy"]) < 1e-9
+    np.testing.assert_allclose(out["best_params"], g["best_params"], atol=1e-6)
+    eng.close()
+
+
+def test_sample_counts_in_protein_decoder_order(vq):
+    """A 7-qubit computational state with qubit 0 flipped samples as '1000000'
+    (qubit 0 leftmost, the plugin's key order); the decoder's order puts qubit 0
+    rightmost (the reference's readout test, test/tests/test_readout.py:14-15)."""
+    from vqemps import ingest, shim
+    kernel = shim.make_kernel()
+    q = kernel.qalloc(7)
+    kernel.x(q[0])
+    counts = shim.sample(kernel, shots_count=1000)
+    assert dict(counts) == {"1000000": 1000}
+    assert ingest.protein_probabilities(counts) == {"0000001": 1.0}
+    kernel2, theta = shim.make_kernel(float)
+    r = kernel2.qalloc(7)
+    kernel2.x(r[2])
+    kernel2.ry(theta, r[6])
+    counts2 = shim.sample(kernel2, 2.0 * np.arccos(np.sqrt(0.75)), shots_count=4000)
+    probs = ingest.protein_probabilities(counts2)
+    assert set(probs) == {"0000100", "1000100"} and abs(probs["0000100"] - 0.75) < 0.04
