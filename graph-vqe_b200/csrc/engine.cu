@@ -276,6 +276,9 @@ struct vqemps_ctx {
   DevBuf<double> grad_stage;
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
+  // Autotuner decisions shared by plans of one size class: (batch-size bucket,
+  // split or prefix plan, power-of-two bucket of node-sites) -> variant.
+  std::map<int, int> tuned_by_shape;
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
   int grad_mma = 2;                     // gradient levels: 0 SIMT, 1 FP64 DMMA, 2 DMMA with Gauss forward
   int split_mode = -1;                  // split evaluation: -1 when it saves work, 0 never, 1 always
@@ -1017,11 +1020,31 @@ static int batch_bucket(int B) {
 // Variant for (plan, batch size): forced, cached, or measured now. Tuning
 // times every variant once on the prepared states (CUDA events, synchronising
 // the stream once per plan and batch-size bucket) and keeps the fastest.
+// A plan's size class for the autotuner: its batch-size bucket, split or prefix
+// evaluation, and the power-of-two bucket of its node-sites per state. Which
+// kernel is fastest follows from these (how many groups a level launch has per
+// state, and how many states share it), so a decision made on one plan is reused
+// for the next plan of the same class instead of timing every variant again --
+// the usual case when a solver loads one Hamiltonian after another.
+static int shape_key(const Hamiltonian &h, int B) {
+  const long long sites = h.cut >= 0 ? h.split_node_sites : h.node_sites;
+  int lg = 0;
+  while ((1LL << lg) < std::max(sites, 1LL)) ++lg;
+  return (batch_bucket(B) * 2 + (h.cut >= 0 ? 1 : 0)) * 64 + lg;
+}
+
 static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int *variant) {
   if (ctx->forced_variant >= 0) { *variant = ctx->forced_variant; return VQEMPS_OK; }
   const int key = batch_bucket(B);
   auto it = h.tuned.find(key);
   if (it != h.tuned.end()) { *variant = it->second; return VQEMPS_OK; }
+  const int skey = shape_key(h, B);
+  auto sit = ctx->tuned_by_shape.find(skey);
+  if (sit != ctx->tuned_by_shape.end()) {
+    h.tuned[key] = sit->second;
+    *variant = sit->second;
+    return VQEMPS_OK;
+  }
   // the two timing events are destroyed on every exit path
   struct Events {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1047,6 +1070,7 @@ static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
     if (ms < best_ms) { best_ms = ms; best = v; }
   }
   h.tuned[key] = best;
+  ctx->tuned_by_shape[skey] = best;
   *variant = best;
   return VQEMPS_OK;
 }

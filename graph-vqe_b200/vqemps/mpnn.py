@@ -49,24 +49,43 @@ def graph_features(n, words, coeffs):
         arr = np.full((0, n), ord("I"), dtype=np.uint8)
     act = arr != ord("I")
     isz = arr == ord("Z")
-    weight = act.sum(1)
-    s = (np.abs(coeffs)[:, None] * act).sum(0)
-    one = (weight == 1) & (isz.sum(1) == 1)
-    h = (coeffs[one, None] * isz[one]).sum(0)
-    # pair sums over every pair of active qubits of every term, one weight class at a time
-    Wt = np.zeros((n, n))
-    Jm = np.zeros((n, n))
-    zz = (weight == 2) & (isz.sum(1) == 2)
+    # active (term, qubit) pairs in row-major order: each term's qubits are
+    # contiguous and ascending, starting at first[t]
+    rows, cols = np.nonzero(act)
+    weight = np.bincount(rows, minlength=T)
+    nz = np.bincount(rows, weights=isz[rows, cols], minlength=T)
+    first = np.cumsum(weight) - weight
     absc = np.abs(coeffs)
+    # per-qubit sums of |c| accumulate in term order, as an axis-0 sum does
+    s = np.bincount(cols, weights=absc[rows], minlength=n) if T else np.zeros(n)
+    one = (weight == 1) & (nz == 1)
+    h = np.zeros(n)
+    if one.any():
+        h = np.bincount(cols[first[one]], weights=coeffs[one], minlength=n)
+    # pair sums over every pair of active qubits of every term, one weight class at
+    # a time; each cell accumulates its contributions in this order, in one
+    # bincount over the concatenated (cell, value) lists
+    zz = (weight == 2) & (nz == 2)
+    w_cells, w_vals, j_cells, j_vals = [], [], [], []
     for wgt in np.unique(weight[weight >= 2]):
         sel = np.nonzero(weight == wgt)[0]
-        q = np.nonzero(act[sel])[1].reshape(len(sel), wgt)       # active qubits, ascending per term
+        q = cols[first[sel][:, None] + np.arange(wgt)[None, :]]   # active qubits, ascending per term
         for i in range(wgt):
             for j in range(i + 1, wgt):
-                np.add.at(Wt, (q[:, i], q[:, j]), absc[sel])
+                w_cells.append(q[:, i] * n + q[:, j])
+                w_vals.append(absc[sel])
         if wgt == 2:
             z = zz[sel]
-            np.add.at(Jm, (q[z, 0], q[z, 1]), coeffs[sel][z])
+            j_cells.append(q[z, 0] * n + q[z, 1])
+            j_vals.append(coeffs[sel][z])
+
+    def cell_sums(cells, vals):
+        if not cells:
+            return np.zeros((n, n))
+        return np.bincount(np.concatenate(cells), weights=np.concatenate(vals), minlength=n * n).reshape(n, n)
+
+    Wt = cell_sums(w_cells, w_vals)
+    Jm = cell_sums(j_cells, j_vals)
     pairs = set(zip(*np.nonzero(np.triu(Wt, 1) > 0))) | {(q, q + 1) for q in range(n - 1)}
     pairs = sorted((int(a), int(b)) for a, b in pairs)
     node = np.stack([slog(h) / SCALE_FIELD, slog(s) / SCALE_WEIGHT, np.arange(n) / max(n - 1, 1),

@@ -96,6 +96,7 @@ class LearnedWarmStart:
         t0 = time.perf_counter()
         # the global problem only: the learned path needs no partition plan
         strat = GlobalProblem(self.engine, n, words, coeffs, energy_tol=energy_tol)
+        t_setup = time.perf_counter() - t0
         P = strat.num_params
         theta = self.propose(n, words, coeffs)
         t_prop = time.perf_counter() - t0
@@ -142,6 +143,7 @@ class LearnedWarmStart:
             reached = trace[-1][0]
             best = trace[-1][1]
         return dict(fallback=False, start=start, proposal_energy=e_prop, zero_energy=e_zero, proposal_s=t_prop,
+                    setup_s=t_setup,
                     best_energy=min(best, min(e for _, e in trace)), reached_s=reached,
                     wall_s=time.perf_counter() - t0, trace=trace)
 
@@ -242,7 +244,9 @@ def evaluate(params_path, count=20, seed0=900000, n=96, terms=40000, global_maxi
                    plain_local_s=plain["local_s"], warm_start_energy=plain["warm_start_energy"],
                    learned_fallback=lw["fallback"], learned_start=lw["start"], proposal_energy=lw["proposal_energy"],
                    zero_energy=lw["zero_energy"], learned_best=lw.get("best_energy"),
-                   learned_reached_s=lw.get("reached_s"), learned_wall_s=lw["wall_s"])
+                   learned_reached_s=lw.get("reached_s"), learned_wall_s=lw["wall_s"],
+                   learned_setup_s=lw.get("setup_s"), learned_proposal_s=lw.get("proposal_s"),
+                   plain_setup_s=plain["setup_s"])
         row["ratio"] = (row["learned_reached_s"] / row["plain_s"]) if row["learned_reached_s"] else None
         rows.append(row)
         print(json.dumps(row), flush=True)
