@@ -292,18 +292,25 @@ def main():
     from vqemps import profiling
     phases = profiling.phase_times(eng, ham, th, repeats=3)
     level_s = phases["levels_s"]
-    flops_step = stats["flops"] * args.batch
-    achieved = flops_step / level_s / 1e12
     variant = eng.level_variant(ham, args.batch)
+    # executed work: the complex kernels' count (8 real flops per complex
+    # multiply-add); the real-arithmetic kernel does one real multiply-add (2
+    # flops) where they do a complex one
+    flops_eval = stats["flops"] / 4.0 if variant == "real_pf" else stats["flops"]
+    flops_step = flops_eval * args.batch
+    achieved = flops_step / level_s / 1e12
     kernel = {"simt": "level_kernel (FP64 FMA pipes)", "simt_pf": "level_pf_kernel (FP64 FMA pipes, cp.async prefetch)",
               "dmma4": "level_mma_kernel<4> (FP64 DMMA tensor cores)",
               "dmma8": "level_mma_kernel<8> (FP64 DMMA tensor cores)",
               "dmma_pf": "level_mma_pf_kernel (FP64 DMMA tensor cores, cp.async parent prefetch)",
               "dmma3_pf": "level_mma3_pf_kernel (FP64 DMMA tensor cores, Gauss 3-product complex multiply, "
-                          "cp.async parent prefetch)"}.get(variant,
+                          "cp.async parent prefetch)",
+              "real_pf": "level_real_pf_kernel (FP64 DMMA tensor cores, real arithmetic with Y-count phases for "
+                         "real-amplitude states, cp.async parent prefetch)"}.get(variant,
                                                                                                     str(variant))
     traffic = profiled_traffic(variant)
-    roofline = dict(bound="tensor" if variant and variant.startswith("dmma") else "fp64", achieved=achieved,
+    roofline = dict(bound="tensor" if variant and variant != "simt" and variant != "simt_pf" else "fp64",
+                    achieved=achieved,
                     peak=fp64_peak, unit="TFLOP/s", frac=achieved / fp64_peak,
                     traffic=traffic * args.batch if traffic else None,
                     kernel=kernel + ", all trie levels of one step",
@@ -349,7 +356,7 @@ def main():
                     config=dict(WORKLOAD, global_batch=args.batch * world, parallelism=f"replicas x{world}",
                                 l2="working set per step > L2 (env buffers ~4 GB): no flush needed",
                                 plain_evals_per_s=plain_rate, batched_over_plain=value / world / plain_rate,
-                                flops_per_eval=stats["flops"], survey_flops_per_eval=stats["flops_survey"],
+                                flops_per_eval=flops_eval, survey_flops_per_eval=stats["flops_survey"],
                                 trie_node_sites=stats["node_sites"], phases_ms=phases["ms"],
                                 golden_gate=gate),
                     roofline=roofline, cpu_baseline=cpu, e2e=e2e,

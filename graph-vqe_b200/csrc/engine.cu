@@ -19,6 +19,7 @@
 #include "evolve.cuh"
 #include "expect.cuh"
 #include "expect_mma.cuh"
+#include "expect_real.cuh"
 #include "sample.cuh"
 #include "gradient.cuh"
 #include "gradient_mma.cuh"
@@ -68,7 +69,8 @@ struct Hamiltonian {
   // prefix environment after site c-1 with a suffix environment of sites c..n-1
   // from a suffix trie (one 16 x 16 dot product per distinct pair).
   int cut = -1;
-  std::vector<int32_t> term_slot;        // T x n: env slot of term t's prefix node at level s (-1 none)
+  std::vector<int32_t> term_slot;        // n x T: env slot of term t's prefix node at level s (-1 none);
+                                         // released once the split plan is built
   std::vector<double> level_flops;       // prefix trie flops per level
   std::vector<DevGroup> sl_groups;       // prefix levels 0..cut-1 with split leaf ids
   std::vector<DevNode> sl_nodes;
@@ -85,20 +87,19 @@ struct Hamiltonian {
   DevGroup *d_sl_groups = nullptr, *d_sr_groups = nullptr;
   DevNode *d_sl_nodes = nullptr, *d_sr_nodes = nullptr;
   int32_t *d_pairs = nullptr, *d_split_term_leaf = nullptr;
+  // Re(i^(prefix phase + suffix phase)) of every pair (pairs' order): the factor a
+  // pair closure of two real-part environments takes (0 for an odd Y count)
+  std::vector<double> pair_sign;
+  double *d_pair_sign = nullptr;
   double *d_split_leaf_coef = nullptr;
   // Pair cotangents of the split gradient, summed in a fixed order: the pairs of
   // prefix slot j are pl_off[j] .. pl_off[j+1]-1 (pairs are sorted by prefix
   // slot); those of suffix slot r are pr_idx[pr_off[r] .. pr_off[r+1]-1].
   std::vector<int32_t> pl_off, pr_off, pr_idx;
   int32_t *d_pl_off = nullptr, *d_pr_off = nullptr, *d_pr_idx = nullptr;
-  ~Hamiltonian() {
-    cudaFree(d_groups); cudaFree(d_nodes); cudaFree(d_leaf_coef); cudaFree(d_term_leaf);
-    cudaFree(d_zmask); cudaFree(d_offdiag); cudaFree(d_codes); cudaFree(d_coeffs);
-    cudaFree(d_sumidx_shared); cudaFree(d_sumidx_word); cudaFree(d_wordlist);
-    cudaFree(d_sl_groups); cudaFree(d_sr_groups); cudaFree(d_sl_nodes); cudaFree(d_sr_nodes);
-    cudaFree(d_pairs); cudaFree(d_split_term_leaf); cudaFree(d_split_leaf_coef);
-    cudaFree(d_pl_off); cudaFree(d_pr_off); cudaFree(d_pr_idx);
-  }
+  // every d_ array above is a slice of this one device allocation
+  unsigned char *d_arena = nullptr;
+  ~Hamiltonian() { cudaFree(d_arena); }
   // leaves of the energy path (split plan when cut >= 0)
   int e_nleaf() const { return cut >= 0 ? split_nleaf : nleaf; }
   int e_identity_leaf() const { return cut >= 0 ? split_identity_leaf : identity_leaf; }
@@ -243,6 +244,9 @@ struct vqemps_ctx {
   // circuit
   int n = 0, P = 0, site_order = 0;
   bool have_circuit = false;
+  // every gate real (and the initial state real): the states have real
+  // amplitudes and the real-arithmetic level kernels may run
+  bool real_circuit = false;
   bool doubling_ok = false;             // only adjacent CX two-qubit gates (gradient path)
   std::vector<DevGate> gates;
   std::vector<cplx> mats;
@@ -451,6 +455,7 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
   std::vector<int> bonds(n + 1, 1);
   int P = 0;
   bool doubling_ok = true;
+  bool real = true;        // RY, H, X, Z, CX, SWAP and real U1 / U2 matrices keep amplitudes real
   const int maxb = ctx->max_bond;
   auto add_two = [&](int s, int mat) {
     DevGate g{};
@@ -469,6 +474,9 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
       GradOp go{};
       go.kind = GOP_ONE; go.site = g.site; go.param = -1; go.angle = op.angle; go.mat = -1;
       go.rot = ROT_NONE;
+      if (op.kind == VQEMPS_RX || op.kind == VQEMPS_RZ || op.kind == VQEMPS_Y || op.kind == VQEMPS_S ||
+          op.kind == VQEMPS_SDG)
+        real = false;
       if (op.kind <= VQEMPS_RZ) {
         g.rot = op.kind == VQEMPS_RX ? ROT_X : op.kind == VQEMPS_RY ? ROT_Y : ROT_Z;
         g.param = op.param;
@@ -479,6 +487,8 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
           return fail(ctx, VQEMPS_INVALID, "U1 matrix index out of range");
         cplx m[4];
         for (int i = 0; i < 4; ++i) m[i] = cmake(matrices[2 * (op.matrix + i)], matrices[2 * (op.matrix + i) + 1]);
+        for (int i = 0; i < 4; ++i)
+          if (m[i].y != 0.0) real = false;
         push_matrix(mats, m, 4, &g.mat);
         go.mat = g.mat;
       } else {
@@ -509,8 +519,10 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
     } else {
       if (op.matrix < 0 || op.matrix + 16 > nmatrices)
         return fail(ctx, VQEMPS_INVALID, "U2 matrix index out of range");
-      for (int i = 0; i < 16; ++i)
+      for (int i = 0; i < 16; ++i) {
         g4[i] = cmake(matrices[2 * (op.matrix + i)], matrices[2 * (op.matrix + i) + 1]);
+        if (g4[i].y != 0.0) real = false;
+      }
     }
     int a = site_of[op.q0], bsite = site_of[op.q1];
     if (a > bsite) {  // swapOperands (sharded_mps.cuh:555-562)
@@ -575,6 +587,7 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
   ctx->init1 = init1;
   ctx->doubling_ok = doubling_ok;
   ctx->have_circuit = true;
+  ctx->real_circuit = real;
   if (ctx->doubling_ok) ctx->doubling_ok = build_site_events(ctx);
   if (ctx->doubling_ok) {
     const int rc = upload_site_events(ctx);
@@ -679,10 +692,11 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
     if (last[t] >= 0) active.push_back(t);
   std::vector<int> parent_node(active.size(), -1);   // node id at the previous level
   std::vector<int> prev_slot;                        // env slot of each node of the previous level
+  std::vector<int> prev_phase;                       // Y-count phase of each node of the previous level
   h->group_off.assign(n + 1, 0);
   h->node_off.assign(n + 1, 0);
   h->nslot.assign(n, 0);
-  h->term_slot.assign((size_t)T * n, -1);
+  h->term_slot.assign((size_t)n * T, -1);   // level-major: one level's writes stay in one row
   h->level_flops.assign(n, 0.0);
   const std::vector<int> &bd = ctx->bonds;
   for (int s = 0; s < n; ++s) {
@@ -701,6 +715,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         cur_node = level_nodes++;
         DevNode nd{};
         nd.code = c; nd.env_slot = -1; nd.leaf = -1;
+        nd.phase = ((s == 0 ? 0 : prev_phase[parent_node[j]]) + (c == 2 ? 1 : 0)) & 3;
         h->nodes.push_back(nd);
         node_has_child.push_back(0);
         prev_parent = parent_node[j];
@@ -731,7 +746,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         h->nodes[h->node_off[s] + k].env_slot = slot_of[k];
       }
     h->nslot[s] = slots;
-    for (size_t j = 0; j < active.size(); ++j) h->term_slot[(size_t)active[j] * n + s] = slot_of[node_of[j]];
+    for (size_t j = 0; j < active.size(); ++j) h->term_slot[(size_t)s * T + active[j]] = slot_of[node_of[j]];
     h->max_slot = std::max(h->max_slot, slots);
     // groups: consecutive nodes with the same parent
     {
@@ -766,43 +781,63 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
       }
     }
     prev_slot = slot_of;
+    prev_phase.resize(level_nodes);
+    for (int k = 0; k < level_nodes; ++k) prev_phase[k] = h->nodes[h->node_off[s] + k].phase;
     active.swap(next_active);
     parent_node.swap(next_parent);
   }
   h->group_off[n] = (int)h->groups.size();
   h->node_off[n] = (int)h->nodes.size();
   build_split_plan(*h, code, last, ctx->bonds, ctx->split_mode);
-  // upload
-  auto up = [&](auto *&dst, const auto &vec) -> cudaError_t {
-    using E = typename std::remove_reference<decltype(vec)>::type::value_type;
-    cudaError_t e = cudaMalloc(&dst, std::max<size_t>(vec.size(), 1) * sizeof(E));
-    if (e != cudaSuccess) return e;
-    if (!vec.empty()) e = cudaMemcpy(dst, vec.data(), vec.size() * sizeof(E), cudaMemcpyHostToDevice);
-    return e;
-  };
-  CUDA_TRY(ctx, up(h->d_groups, h->groups));
-  CUDA_TRY(ctx, up(h->d_nodes, h->nodes));
-  CUDA_TRY(ctx, up(h->d_leaf_coef, h->leaf_coef));
-  CUDA_TRY(ctx, up(h->d_term_leaf, h->term_leaf));
-  CUDA_TRY(ctx, up(h->d_zmask, h->zmask));
-  CUDA_TRY(ctx, up(h->d_offdiag, h->offdiag));
+  std::vector<int32_t>().swap(h->term_slot);
+  // upload: every plan array is a 256-byte aligned slice of ONE device
+  // allocation, filled by one copy of a packed host image (tens of separate
+  // allocations and copies cost more than the plan build itself at 40,000 terms)
   h->codes = std::move(code);
-  CUDA_TRY(ctx, up(h->d_codes, h->codes));
-  CUDA_TRY(ctx, up(h->d_coeffs, h->coeffs));
-  CUDA_TRY(ctx, up(h->d_sumidx_shared, sumidx_shared));
-  CUDA_TRY(ctx, up(h->d_sumidx_word, sumidx_word));
-  CUDA_TRY(ctx, up(h->d_wordlist, wl));
+  struct Slice {
+    void **dst;
+    const void *src;
+    size_t bytes, off;
+  };
+  std::vector<Slice> slices;
+  size_t total = 0;
+  auto add = [&](auto *&dst, const auto &vec) {
+    using E = typename std::remove_reference<decltype(vec)>::type::value_type;
+    const size_t bytes = vec.size() * sizeof(E);
+    slices.push_back({reinterpret_cast<void **>(&dst), vec.data(), bytes, total});
+    total += (std::max<size_t>(bytes, sizeof(E)) + 255) & ~(size_t)255;
+  };
+  add(h->d_groups, h->groups);
+  add(h->d_nodes, h->nodes);
+  add(h->d_leaf_coef, h->leaf_coef);
+  add(h->d_term_leaf, h->term_leaf);
+  add(h->d_zmask, h->zmask);
+  add(h->d_offdiag, h->offdiag);
+  add(h->d_codes, h->codes);
+  add(h->d_coeffs, h->coeffs);
+  add(h->d_sumidx_shared, sumidx_shared);
+  add(h->d_sumidx_word, sumidx_word);
+  add(h->d_wordlist, wl);
   if (h->cut >= 0) {
-    CUDA_TRY(ctx, up(h->d_sl_groups, h->sl_groups));
-    CUDA_TRY(ctx, up(h->d_sl_nodes, h->sl_nodes));
-    CUDA_TRY(ctx, up(h->d_sr_groups, h->sr_groups));
-    CUDA_TRY(ctx, up(h->d_sr_nodes, h->sr_nodes));
-    CUDA_TRY(ctx, up(h->d_pairs, h->pairs));
-    CUDA_TRY(ctx, up(h->d_split_leaf_coef, h->split_leaf_coef));
-    CUDA_TRY(ctx, up(h->d_split_term_leaf, h->split_term_leaf));
-    CUDA_TRY(ctx, up(h->d_pl_off, h->pl_off));
-    CUDA_TRY(ctx, up(h->d_pr_off, h->pr_off));
-    CUDA_TRY(ctx, up(h->d_pr_idx, h->pr_idx));
+    add(h->d_sl_groups, h->sl_groups);
+    add(h->d_sl_nodes, h->sl_nodes);
+    add(h->d_sr_groups, h->sr_groups);
+    add(h->d_sr_nodes, h->sr_nodes);
+    add(h->d_pairs, h->pairs);
+    add(h->d_split_leaf_coef, h->split_leaf_coef);
+    add(h->d_split_term_leaf, h->split_term_leaf);
+    add(h->d_pl_off, h->pl_off);
+    add(h->d_pr_off, h->pr_off);
+    add(h->d_pr_idx, h->pr_idx);
+    add(h->d_pair_sign, h->pair_sign);
+  }
+  {
+    std::vector<unsigned char> image(total, 0);
+    for (const Slice &sl : slices)
+      if (sl.bytes) std::memcpy(image.data() + sl.off, sl.src, sl.bytes);
+    CUDA_TRY(ctx, cudaMalloc(&h->d_arena, std::max<size_t>(total, 256)));
+    for (const Slice &sl : slices) *sl.dst = h->d_arena + sl.off;
+    CUDA_TRY(ctx, cudaMemcpy(h->d_arena, image.data(), total, cudaMemcpyHostToDevice));
   }
   const int id = ctx->next_handle++;
   ctx->hams[id] = std::move(h);
@@ -904,7 +939,11 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
 }
 
 // Level kernel variants: the autotuner times each on the caller's workload.
-enum : int { LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5, LV_COUNT = 6 };
+enum : int {
+  LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5,
+  LV_REALPF4 = 6,   // real arithmetic: circuits of real gates only
+  LV_COUNT = 7
+};
 
 // Parents per warp of the prefetch DMMA kernels: 8 on wide levels, 4 on
 // middling ones, fewer while the whole batch would give less than two waves of
@@ -943,6 +982,12 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
       level_mma3_pf_kernel<<<dim3(ctas, B), MPF_WARPS * 32, sizeof(LevelMmaPfSmem), st>>>(lp, gpw);
       break;
     }
+    case LV_REALPF4: {
+      const int gpw = mpf_parents_per_warp(ng, B, sms);
+      const int ctas = (ng + RL_WARPS * gpw - 1) / (RL_WARPS * gpw);
+      level_real_pf_kernel<<<dim3(ctas, B), RL_WARPS * 32, sizeof(LevelRealSmem), st>>>(lp, gpw);
+      break;
+    }
     default:
       level_kernel<<<dim3((ng + LEVEL_WARPS - 1) / LEVEL_WARPS, B), LEVEL_WARPS * 32, sizeof(LevelSmem), st>>>(lp);
   }
@@ -950,6 +995,8 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
 
 // All trie levels of one evaluation with a given variant (needs launch_right first).
 static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int variant) {
+  if (variant == LV_REALPF4 && !ctx->real_circuit)
+    return fail(ctx, VQEMPS_INVALID, "the real-arithmetic level kernels need a circuit of real gates");
   const int n = ctx->n;
   const int nleaf = std::max(h.e_nleaf(), 1);
   const bool split = h.cut >= 0;
@@ -977,7 +1024,8 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       lp.n = n;
       lp.s = s;
       lp.suffix = 1;
-      launch_level_variant(variant == LV_MMA3PF4 ? LV_MMA3PF4 : LV_MMAPF4, lp, ng, B, ctx->sm_count, st);
+      launch_level_variant(variant == LV_MMA3PF4 || variant == LV_REALPF4 ? variant : LV_MMAPF4, lp, ng, B,
+                           ctx->sm_count, st);
       CUDA_TRY(ctx, cudaGetLastError());
     }
   }
@@ -1003,9 +1051,17 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     CUDA_TRY(ctx, cudaGetLastError());
   }
   if (split && h.npairs > 0) {
-    split_combine_kernel<<<dim3((h.npairs + COMBINE_WARPS - 1) / COMBINE_WARPS, B), COMBINE_WARPS * 32, 0, st>>>(
-        envs[(h.cut - 1) & 1], std::max(h.nslot[h.cut - 1], 1), (h.cut & 1) ? ctx->env3.ptr : ctx->env2.ptr,
-        std::max(h.sr_nslot[h.cut], 1), h.d_pairs, h.npairs, ctx->status.ptr, ctx->leafval.ptr, nleaf);
+    const dim3 grid((h.npairs + COMBINE_WARPS - 1) / COMBINE_WARPS, B);
+    cplx *left = envs[(h.cut - 1) & 1], *right = (h.cut & 1) ? ctx->env3.ptr : ctx->env2.ptr;
+    if (variant == LV_REALPF4)
+      split_combine_real_kernel<<<grid, COMBINE_WARPS * 32, 0, st>>>(
+          reinterpret_cast<const double *>(left), std::max(h.nslot[h.cut - 1], 1),
+          reinterpret_cast<const double *>(right), std::max(h.sr_nslot[h.cut], 1), h.d_pairs, h.d_pair_sign,
+          h.npairs, ctx->status.ptr, ctx->leafval.ptr, nleaf);
+    else
+      split_combine_kernel<<<grid, COMBINE_WARPS * 32, 0, st>>>(
+          left, std::max(h.nslot[h.cut - 1], 1), right, std::max(h.sr_nslot[h.cut], 1), h.d_pairs, h.npairs,
+          ctx->status.ptr, ctx->leafval.ptr, nleaf);
     CUDA_TRY(ctx, cudaGetLastError());
   }
   return VQEMPS_OK;
@@ -1058,6 +1114,7 @@ static int pick_variant(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st,
   int best = LV_SIMT4;
   float best_ms = 1e30f;
   for (int v = 0; v < LV_COUNT; ++v) {
+    if (v == LV_REALPF4 && !ctx->real_circuit) continue;   // complex amplitudes
     int rc = run_levels(ctx, h, B, st, v);      // warm
     if (rc) return rc;
     CUDA_TRY(ctx, cudaEventRecord(ev.e0, st));

@@ -33,7 +33,9 @@ struct DevNode {    // one trie node
   int32_t code;          // 0 I, 1 X, 2 Y, 3 Z
   int32_t env_slot;      // slot in this level's env buffer, -1 if no descendants
   int32_t leaf;          // leaf id if a term ends here, else -1
-  int32_t pad;
+  int32_t phase;         // number of Y codes on the node's path, mod 4: for a state
+                         // with real amplitudes the node's environment is i^phase
+                         // times a real matrix (the real-arithmetic levels use it)
 };
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,261 @@
+// Trie levels in real arithmetic, for states whose amplitudes are real.
+//
+// When every gate of the circuit is real (RY, CX, X, Z, H, SWAP, real U1/U2) and
+// the initial state is real, every site tensor A and every identity right
+// environment R is real. A trie node's environment is then
+//   E = i^k Er,   k = the number of Y codes on the node's path, mod 4 (DevNode.phase),
+// with Er real: the transfer E' = sum_ij P_ij A_i^H E A_j (analytic_batch.cuh:4-36
+// in the reference, for complex tensors) keeps the factor i^k for I, X and Z and
+// multiplies in i for Y. These levels carry Er only:
+//   I: A0^T Er A0 + A1^T Er A1        Z: A0^T Er A0 - A1^T Er A1
+//   X: A0^T Er A1 + A1^T Er A0        Y: A1^T Er A0 - A0^T Er A1   (phase k + 1)
+// and a term's value Re sum_xy E[x][y] R[x][y] is Re(i^k) sum Er o R: zero for
+// an odd number of Y's, negated for k = 2. E is Hermitian, so Er is symmetric for
+// even k and antisymmetric for odd k; A_x^T Er A_x inherits that, and
+// A1^T Er A0 = +-(A0^T Er A1)^T. As in the complex kernels the class products
+// form three of four 8 x 8 tiles (the (1,0) tile is +-(0,1)^T) and the X/Y pair
+// one product -- but each is ONE real product where the complex kernels issue
+// three (Gauss): 56 DMMA issues per one-class parent instead of 168, and the
+// environments moved between levels are half the bytes.
+//
+// Shared tiles hold doubles, padded so that the fragment loads of a half-warp
+// (lanes g = 0..3 rows, t = 0..3 columns) fall on 16 distinct 8-byte banks:
+// row strides are 4 mod 16 doubles.
+#pragma once
+#include "common.cuh"
+#include "expect.cuh"
+#include "expect_mma.cuh"
+
+namespace vqemps {
+
+constexpr int RL_WARPS = 4;
+constexpr int RL_E_STRIDE = 20;   // E: 16 rows of 16 doubles
+constexpr int RL_A_STRIDE = 36;   // site panel: 16 rows [a] of 32 doubles [i * 16 + c]
+constexpr int RL_S_STRIDE = 20;   // S = Er [A_0 | A_1]: [i][a][c], 2 x 16 rows of 16 doubles
+
+struct LevelRealSmem {
+  double A[CHI * RL_A_STRIDE];
+  double R[ENV_ELEMS];
+  double E[RL_WARPS][CHI * RL_E_STRIDE];
+  double S[RL_WARPS][2 * CHI * RL_S_STRIDE];
+};
+
+// Re(i^k)
+__device__ __forceinline__ double re_ipow(int k) { return (k & 1) ? 0.0 : ((k & 2) ? -1.0 : 1.0); }
+
+// The parent environment of group grp into E: a real environment of the
+// previous level (cp.async, 16 bytes = two doubles per copy), the real part of
+// the identity right environment R_{s+1} for a suffix root, or the 1 x 1 vacuum.
+__device__ __forceinline__ void stage_parent_real(const LevelParams &p, int b, const DevGroup &grp, double *E,
+                                                  int lane) {
+  if (grp.parent_slot < 0 && p.suffix) {
+    const cplx *src = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * RL_E_STRIDE + (e & 15)] = src[e].x;
+  } else if (grp.parent_slot < 0) {
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * RL_E_STRIDE + (e & 15)] = e == 0 ? 1.0 : 0.0;
+  } else {
+    const double *src = reinterpret_cast<const double *>(p.env_prev) +
+                        ((size_t)b * p.nslot_prev + grp.parent_slot) * ENV_ELEMS;
+    for (int e = lane; e < ENV_ELEMS / 2; e += 32) cp_async16(E + (e >> 3) * RL_E_STRIDE + 2 * (e & 7), src + 2 * e);
+  }
+}
+
+// acc = A_x^T S_y over the 8 x 8 output tiles (rt, ct) (x = column offset 0 or
+// CHI of the site panel, y = panel half); SKIP10 leaves the (1,0) tile out.
+template <bool SKIP10>
+__device__ __forceinline__ void class_tiles_real(const double *A, int xoff, const double *S, int y,
+                                                 double (&acc)[2][2][2], int g, int t) {
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct) acc[rt][ct][0] = acc[rt][ct][1] = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks) {
+    double x[2], yv[2];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt) x[rt] = A[(ks * 4 + t) * RL_A_STRIDE + xoff + rt * 8 + g];
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct) yv[ct] = S[(y * CHI + ks * 4 + t) * RL_S_STRIDE + ct * 8 + g];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 2; ++ct) {
+        if (SKIP10 && rt == 1 && ct == 0) continue;
+        dmma(acc[rt][ct][0], acc[rt][ct][1], x[rt], yv[ct]);
+      }
+  }
+}
+
+// One trie level for B states (uniform batch: state blockIdx.y, groups
+// interleaved over the grid, groups_per_warp each), environments as real parts.
+__global__ void __launch_bounds__(RL_WARPS * 32, 4)
+level_real_pf_kernel(LevelParams p, int groups_per_warp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  LevelRealSmem &sm = *reinterpret_cast<LevelRealSmem *>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.y;
+  const int stride = gridDim.x * RL_WARPS;
+  const int first = blockIdx.x * RL_WARPS + warp;
+  int count = 0;
+  if (first < p.ngroups) count = min(groups_per_warp, (p.ngroups - first + stride - 1) / stride);
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += RL_WARPS * 32)
+      sm.A[(e >> 5) * RL_A_STRIDE + (e & 31)] = ag[e].x;
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += RL_WARPS * 32) sm.R[e] = rg[e].x;
+  }
+  __syncthreads();
+  const double *A = sm.A;
+  const double *R = sm.R;
+  double *E = sm.E[warp];
+  double *S = sm.S[warp];
+  double *env_cur = reinterpret_cast<double *>(p.env_cur);
+  const int g = lane >> 2, t = lane & 3;
+  if (count == 0) return;
+  stage_parent_real(p, b, p.groups[first], E, lane);
+  cp_async_commit();
+  for (int k = 0; k < count; ++k) {
+    const int gidx = first + k * stride;
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    // ---- S = Er [A_0 | A_1] (16 x 32): 32 DMMA issues
+    {
+      double sacc[2][4][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) sacc[rt][ct][0] = sacc[rt][ct][1] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        double ef[2], pf[4];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * RL_E_STRIDE + ks * 4 + t];
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) pf[ct] = A[(ks * 4 + t) * RL_A_STRIDE + ct * 8 + g];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) dmma(sacc[rt][ct][0], sacc[rt][ct][1], ef[rt], pf[ct]);
+      }
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int col = ct * 8 + 2 * t + j;
+            S[((col >> 4) * CHI + rt * 8 + g) * RL_S_STRIDE + (col & 15)] = sacc[rt][ct][j];
+          }
+    }
+    __syncwarp();   // Er is dead and S is complete: prefetch the next parent
+    if (k + 1 < count) stage_parent_real(p, b, p.groups[gidx + stride], E, lane);
+    cp_async_commit();
+    // the parent's phase (from its first child): symmetric Er for even, antisymmetric for odd
+    const DevNode first_child = p.nodes[grp.child_begin];
+    const int kp = (first_child.phase - (first_child.code == 2 ? 1 : 0)) & 3;
+    const double sp = (kp & 1) ? -1.0 : 1.0;
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      // I/Z: t0 = A_0^T S_0, t1 = A_1^T S_1 (tiles (0,0), (0,1), (1,1));
+      // X/Y: t0 = A_0^T S_1 (four tiles), t1 = A_1^T S_0 = sp t0^T through the panel
+      double a[2][2][2], c[2][2][2];
+      if (cls == 0) {
+        class_tiles_real<true>(A, 0, S, 0, a, g, t);
+        class_tiles_real<true>(A, CHI, S, 1, c, g, t);
+      } else {
+        class_tiles_real<false>(A, 0, S, 1, a, g, t);
+        __syncwarp();   // the panel is consumed: t0 goes into its place
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) S[(rt * 8 + g) * RL_S_STRIDE + ct * 8 + 2 * t + j] = a[rt][ct][j];
+        __syncwarp();
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) c[rt][ct][j] = sp * S[(ct * 8 + 2 * t + j) * RL_S_STRIDE + rt * 8 + g];
+      }
+      for (int ci = 0; ci < grp.nchild; ++ci) {
+        const DevNode node = p.nodes[grp.child_begin + ci];
+        const bool iz = (node.code == 0 || node.code == 3);
+        if (iz != (cls == 0)) continue;
+        // child symmetry: the (1,0) tile is sc times the transposed (0,1) tile
+        const double sc = (node.phase & 1) ? -1.0 : 1.0;
+        double out[2][2][2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const double t0 = a[rt][ct][j], t1 = c[rt][ct][j];
+              out[rt][ct][j] = (node.code == 0 || node.code == 1) ? t0 + t1 : (node.code == 3 ? t0 - t1 : t1 - t0);
+            }
+        if (node.env_slot >= 0) {
+          double *dst = env_cur + ((size_t)b * p.nslot_cur + node.env_slot) * ENV_ELEMS;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = sc * out[0][1][j];
+        }
+        if (node.leaf >= 0) {
+          const double w = re_ipow(node.phase);
+          double v = 0.0;
+          if (w != 0.0) {
+#pragma unroll
+            for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+              for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) v += out[rt][ct][j] * R[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) v += sc * out[0][1][j] * R[(8 + 2 * t + j) * CHI + g];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          }
+          if (lane == 0) p.leafval[(size_t)b * p.nleaf_total + node.leaf] = w * v;
+        }
+      }
+    }
+    __syncwarp();   // S is rewritten by the next parent
+  }
+  cp_async_wait<0>();
+}
+
+// The pair closures of the split evaluation on real-part environments:
+// value = Re(i^(prefix phase + suffix phase)) sum_xy L[x][y] R[x][y] (pair_sign).
+__global__ void __launch_bounds__(COMBINE_WARPS * 32)
+split_combine_real_kernel(const double *__restrict__ left, int left_nslot, const double *__restrict__ right,
+                          int right_nslot, const int32_t *__restrict__ pairs, const double *__restrict__ pair_sign,
+                          int npairs, const int32_t *__restrict__ status, double *__restrict__ leafval,
+                          int nleaf_total) {
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pidx = blockIdx.x * COMBINE_WARPS + warp;
+  if (pidx >= npairs) return;
+  const int ls = pairs[3 * pidx], rs = pairs[3 * pidx + 1], leaf = pairs[3 * pidx + 2];
+  const double w = pair_sign[pidx];
+  double v = 0.0;
+  if (w != 0.0) {
+    const double2 *L = reinterpret_cast<const double2 *>(left + ((size_t)b * left_nslot + ls) * ENV_ELEMS);
+    const double2 *R = reinterpret_cast<const double2 *>(right + ((size_t)b * right_nslot + rs) * ENV_ELEMS);
+    for (int e = lane; e < ENV_ELEMS / 2; e += 32) {
+      const double2 l = L[e], r = R[e];
+      v = fma(l.x, r.x, v);
+      v = fma(l.y, r.y, v);
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  }
+  if (lane == 0) leafval[(size_t)b * nleaf_total + leaf] = status[b] == 0 ? w * v : 0.0;
+}
+
+}  // namespace vqemps

@@ -201,7 +201,8 @@ class Engine:
     def free_hamiltonian(self, ham: Hamiltonian):
         check(self.ctx, self.lib.vqemps_free_hamiltonian(self.ctx, ham.handle), "free_hamiltonian")
 
-    LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf")
+    # "real_pf": real arithmetic, for circuits of real gates only
+    LEVEL_VARIANTS = ("simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf", "real_pf")
 
     def set_level_variant(self, variant):
         """Force a trie-level kernel (one of LEVEL_VARIANTS) or None to autotune."""

@@ -1,0 +1,114 @@
+"""GPU: the real-arithmetic trie levels (variant "real_pf") for circuits of real
+gates. Environments are carried as real parts with the plan's Y-count phase;
+results must equal the reference's ReverseMPS golden energies (1e-9 relative)
+on every real-gate circuit, including words with X and Y, equal the complex
+DMMA kernels to rounding on the benchmark batch (energies 1e-11 relative,
+per-term values 1e-12), in both the prefix and the split evaluation; complex
+circuits refuse the variant and the autotuner never picks it for them."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reverse_mps_golden.json").read_text())
+LARGE = json.loads((Path(__file__).parent / "golden" / "large_workloads_golden.json").read_text())
+REAL_GATES = {"ry", "cx", "x", "z", "h", "swap"}
+
+
+def _real(case):
+    return all(op[0] in REAL_GATES for op in case["spec"]["ops"])
+
+
+def _spec(case):
+    s = case["spec"]
+    return dict(n=s["n"], ops=[tuple(o) for o in s["ops"]], initial=s["initial"], count=s["count"])
+
+
+@pytest.fixture(scope="module")
+def vq(cuda_device):
+    import vqemps
+    return vqemps
+
+
+@pytest.mark.parametrize("split", ["auto", "off", "on"])
+@pytest.mark.parametrize("order", ["msb", "qubit"])
+@pytest.mark.parametrize("case", [c for c in GOLDEN if _real(c)], ids=lambda c: c["name"])
+def test_real_levels_match_reference_golden(vq, case, order, split):
+    eng = vq.Engine(0, 16)
+    eng.set_split_mode({"auto": None, "off": False, "on": True}[split])
+    eng.set_spec(_spec(case), site_order=order)
+    eng.set_level_variant("real_pf")
+    ham = eng.set_hamiltonian(case["words"], case["coeffs"])
+    e = float(eng.energy(ham, np.array(case["x"]))[0])
+    assert abs(e - case["energy"]) <= 1e-9 * max(1.0, abs(case["energy"]))
+    eng.close()
+
+
+@pytest.mark.parametrize("case", [c for c in GOLDEN if not _real(c)], ids=lambda c: c["name"])
+def test_complex_circuits_refuse_real_levels(vq, case):
+    eng = vq.Engine(0, 16)
+    eng.set_spec(_spec(case))
+    ham = eng.set_hamiltonian(case["words"], case["coeffs"])
+    eng.set_level_variant("real_pf")
+    with pytest.raises(vq.EngineError, match="real gates"):
+        eng.energy(ham, np.array(case["x"]))
+    eng.set_level_variant(None)
+    e = float(eng.energy(ham, np.array(case["x"]))[0])
+    assert abs(e - case["energy"]) <= 1e-9 * max(1.0, abs(case["energy"]))
+    assert eng.level_variant(ham, 1) != "real_pf"
+    eng.close()
+
+
+def test_real_levels_with_x_and_y_words(vq):
+    """H gates make X and Y expectations nonzero (even numbers of Y's); odd
+    numbers of Y's vanish for real amplitudes. Per-term values against the
+    complex kernel."""
+    from oracle import mps_oracle as O
+    n = 10
+    spec = O.hardware_efficient_spec(n, 3, ("ry",), "linear")
+    spec["ops"] = [("h", q) for q in range(n)] + list(spec["ops"])
+    rng = np.random.default_rng(9)
+    words = ["".join(rng.choice(list("IXYZ"), n, p=[0.55, 0.15, 0.15, 0.15])) for _ in range(400)]
+    words += ["YY" + "I" * (n - 2), "Y" + "I" * (n - 1), "XYXYIIIIII", "IIIIIIIIII"]
+    coeffs = rng.normal(size=len(words))
+    x = rng.uniform(-np.pi, np.pi, (3, spec["count"]))
+    out = {}
+    for variant in ("real_pf", "dmma3_pf"):
+        for split in (False, True):
+            eng = vq.Engine(0, 16)
+            eng.set_split_mode(split)
+            eng.set_spec(spec)
+            eng.set_level_variant(variant)
+            ham = eng.set_hamiltonian(words, coeffs)
+            e, pt = eng.energy(ham, torch.tensor(x, device=eng.device), per_term=True)
+            out[variant, split] = (e.cpu().numpy(), pt.cpu().numpy())
+            eng.close()
+    ref_e, ref_pt = out["dmma3_pf", False]
+    psi = O.dense_statevector(spec, x[0])
+    dense = O.dense_expectations(psi, words).real
+    np.testing.assert_allclose(ref_pt[0], dense, atol=1e-11)
+    for key, (e, pt) in out.items():
+        np.testing.assert_allclose(e, ref_e, rtol=1e-11, atol=1e-11)
+        np.testing.assert_allclose(pt, ref_pt, rtol=0, atol=1e-12)
+    odd = [i for i, w in enumerate(words) if w.count("Y") % 2 == 1]
+    assert np.all(out["real_pf", True][1][:, odd] == 0.0)
+
+
+def test_real_levels_on_the_benchmark_batch(vq):
+    from vqemps import workloads as VW
+    spec, words, coeffs, thetas = VW.batched_40q(seed=0, batch=256)
+    g = LARGE["batched_40q"]
+    out = {}
+    for variant in ("real_pf", "dmma3_pf"):
+        eng = vq.Engine(0, 16)
+        eng.set_spec(spec)
+        eng.set_level_variant(variant)
+        ham = eng.set_hamiltonian(words, coeffs)
+        out[variant] = eng.energy(ham, torch.tensor(thetas, device=eng.device)).cpu().numpy()
+        eng.close()
+    for i, ref in zip(g["indices"], g["energies"]):
+        assert abs(out["real_pf"][i] - ref) <= 1e-9 * max(1.0, abs(ref))
+    np.testing.assert_allclose(out["real_pf"], out["dmma3_pf"], rtol=1e-11, atol=1e-9)
