@@ -38,6 +38,6 @@ __device__ __forceinline__ void cfma_conj(cplx &acc, cplx a, cplx b) {
 __device__ __forceinline__ double cabs2(cplx a) { return a.x * a.x + a.y * a.y; }
 
 // Status words written by kernels (mirrors vqemps_status).
-enum : int32_t { ST_OK = 0, ST_INSUFFICIENT = 1, ST_NONFINITE = 2, ST_INVALID = 3 };
+enum : int32_t { ST_OK = 0, ST_INSUFFICIENT = 1, ST_NONFINITE = 2, ST_INVALID = 3, ST_TIMEOUT = 5 };
 
 }  // namespace vqemps

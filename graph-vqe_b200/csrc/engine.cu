@@ -236,6 +236,13 @@ struct DevBuf {
 
 }  // namespace
 
+// Trie-level kernel variants (the autotuner's candidates).
+enum : int {
+  LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5,
+  LV_REALPF4 = 6,   // real arithmetic: circuits of real gates only
+  LV_COUNT = 7
+};
+
 struct vqemps_ctx {
   int device = 0;
   int max_bond = 16;
@@ -269,6 +276,7 @@ struct vqemps_ctx {
   DevBuf<cplx> sites, right, env0, env1, env2, env3, sites_t;
   DevBuf<int32_t> bonds_ws, status;
   DevBuf<double> leafval, theta_stage, energy_stage, per_term_stage;
+  DevBuf<double> panels, panels_t, right_real;   // real-arithmetic levels: real site panels, real R
   DevBuf<uint64_t> bits, seeds;
   DevBuf<int32_t> zsum;
   DevBuf<cplx> branch;
@@ -360,8 +368,8 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the
   // autotuner's timings are meaningless under a serialising profiler.
   if (const char *v = std::getenv("VQEMPS_LEVEL_VARIANT")) {
-    static const char *names[] = {"simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf"};
-    for (int i = 0; i < 6; ++i)
+    static const char *names[LV_COUNT] = {"simt", "dmma4", "dmma8", "simt_pf", "dmma_pf", "dmma3_pf", "real_pf"};
+    for (int i = 0; i < LV_COUNT; ++i)
       if (std::strcmp(v, names[i]) == 0 || (v[0] == '0' + i && v[1] == 0)) ctx->forced_variant = i;
   }
   *out = ctx;
@@ -939,11 +947,6 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
 }
 
 // Level kernel variants: the autotuner times each on the caller's workload.
-enum : int {
-  LV_SIMT4 = 0, LV_MMA4 = 1, LV_MMA8 = 2, LV_PF4 = 3, LV_MMAPF4 = 4, LV_MMA3PF4 = 5,
-  LV_REALPF4 = 6,   // real arithmetic: circuits of real gates only
-  LV_COUNT = 7
-};
 
 // Parents per warp of the prefetch DMMA kernels: 8 on wide levels, 4 on
 // middling ones, fewer while the whole batch would give less than two waves of
@@ -1001,10 +1004,29 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
   const int nleaf = std::max(h.e_nleaf(), 1);
   const bool split = h.cut >= 0;
   const int top = split ? h.cut : n;                // prefix levels run on sites 0 .. top - 1
+  const bool real = variant == LV_REALPF4;
+  if (real) {
+    // real site panels (and transposed ones for the suffix levels) and real R
+    CUDA_TRY(ctx, ctx->panels.ensure((size_t)B * n * RL_PANEL));
+    CUDA_TRY(ctx, ctx->right_real.ensure((size_t)B * (n + 1) * ENV_ELEMS));
+    real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 0, ctx->panels.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    if (split) {
+      CUDA_TRY(ctx, ctx->panels_t.ensure((size_t)B * n * RL_PANEL));
+      real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 1, ctx->panels_t.ptr);
+      CUDA_TRY(ctx, cudaGetLastError());
+    }
+    const size_t rcount = (size_t)B * (n + 1) * ENV_ELEMS;
+    real_parts_kernel<<<(unsigned)std::min<size_t>((rcount + 255) / 256, 4096), 256, 0, st>>>(ctx->right.ptr, rcount,
+                                                                                           ctx->right_real.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+  }
   if (split) {
     // suffix levels n-1 .. cut on transposed site tensors, starting from R_{l+1}
-    transpose_sites_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
-    CUDA_TRY(ctx, cudaGetLastError());
+    if (!real) {
+      transpose_sites_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
+      CUDA_TRY(ctx, cudaGetLastError());
+    }
     cplx *renv[2] = {ctx->env2.ptr, ctx->env3.ptr};
     for (int s = n - 1; s >= h.cut; --s) {
       const int ng = h.sr_group_off[s + 1] - h.sr_group_off[s];
@@ -1024,6 +1046,9 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       lp.n = n;
       lp.s = s;
       lp.suffix = 1;
+      lp.panels = ctx->panels_t.ptr;
+      lp.right_real = ctx->right_real.ptr;
+      lp.status = ctx->status.ptr;
       launch_level_variant(variant == LV_MMA3PF4 || variant == LV_REALPF4 ? variant : LV_MMAPF4, lp, ng, B,
                            ctx->sm_count, st);
       CUDA_TRY(ctx, cudaGetLastError());
@@ -1047,6 +1072,9 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.nleaf_total = nleaf;
     lp.n = n;
     lp.s = s;
+    lp.panels = ctx->panels.ptr;
+    lp.right_real = ctx->right_real.ptr;
+    lp.status = ctx->status.ptr;
     launch_level_variant(variant, lp, ng, B, ctx->sm_count, st);
     CUDA_TRY(ctx, cudaGetLastError());
   }
@@ -1287,6 +1315,8 @@ extern "C" int vqemps_batch_status(vqemps_ctx *ctx, int32_t *status, int B, void
                " is insufficient for zero-cutoff simulation: resolved singular values would be discarded";
   else if (first == VQEMPS_NONFINITE_SVD)
     ctx->err = "Direct MPS SVD failed or produced nonfinite singular values";
+  else if (first == VQEMPS_TIMEOUT)
+    ctx->err = "a bounded device wait gave up (bulk copy or barrier did not complete)";
   return first;
 }
 

@@ -142,6 +142,13 @@ struct LevelParams {
   // holds transposed site tensors and a group without a parent slot starts from
   // the identity right environment R_{s+1} instead of the vacuum.
   int suffix;
+  // Real-arithmetic levels: real padded site panels [B][n][CHI * 36] doubles
+  // (transposed ones for suffix levels), real parts of the identity right
+  // environments [B][n + 1][ENV_ELEMS], and the per-state status words (a
+  // bounded device wait that gives up writes ST_TIMEOUT there).
+  const double *panels;
+  const double *right_real;
+  int32_t *status;
 };
 
 struct LevelSmem {

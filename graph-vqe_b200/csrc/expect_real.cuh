@@ -21,6 +21,16 @@
 // Shared tiles hold doubles, padded so that the fragment loads of a half-warp
 // (lanes g = 0..3 rows, t = 0..3 columns) fall on 16 distinct 8-byte banks:
 // row strides are 4 mod 16 doubles.
+//
+// Tile movement is by the bulk-copy (TMA) engine: real_panels_kernel writes every
+// site tensor once per step as a real panel already in the padded shared-memory
+// layout, so a CTA stages its site panel and right environment with two 1-D
+// cp.async.bulk copies (4,608 + 2,048 bytes), and each warp fetches the next
+// parent environment with 16 row copies of 128 bytes into its padded tile; all
+// complete on mbarriers (expect_tx), one per CTA and one per warp. Sources are
+// this GPU's memory, addresses 16-byte aligned, sizes multiples of 16, and no
+// copy uses cluster multicast. Every wait is bounded: a wait that gives up marks
+// the state ST_TIMEOUT, waits once more (bounded) for its copies and returns.
 #pragma once
 #include "common.cuh"
 #include "expect.cuh"
@@ -33,30 +43,78 @@ constexpr int RL_E_STRIDE = 20;   // E: 16 rows of 16 doubles
 constexpr int RL_A_STRIDE = 36;   // site panel: 16 rows [a] of 32 doubles [i * 16 + c]
 constexpr int RL_S_STRIDE = 20;   // S = Er [A_0 | A_1]: [i][a][c], 2 x 16 rows of 16 doubles
 
+constexpr int RL_PANEL = CHI * RL_A_STRIDE;   // doubles per real site panel (4,608 bytes)
+
 struct LevelRealSmem {
-  double A[CHI * RL_A_STRIDE];
+  double A[RL_PANEL];
   double R[ENV_ELEMS];
   double E[RL_WARPS][CHI * RL_E_STRIDE];
   double S[RL_WARPS][2 * CHI * RL_S_STRIDE];
+  uint64_t bar_cta;                 // site panel + right environment
+  uint64_t bar_warp[RL_WARPS];      // each warp's parent environment
 };
 
 // Re(i^k)
 __device__ __forceinline__ double re_ipow(int k) { return (k & 1) ? 0.0 : ((k & 2) ? -1.0 : 1.0); }
 
-// The parent environment of group grp into E: a real environment of the
-// previous level (cp.async, 16 bytes = two doubles per copy), the real part of
-// the identity right environment R_{s+1} for a suffix root, or the 1 x 1 vacuum.
+// ---- bulk copies completing on an mbarrier ----
+__device__ __forceinline__ unsigned smem_addr(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// generic-proxy accesses of shared memory before a bulk copy overwrites it
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+// Wait until the barrier's phase with the given parity completes; false after
+// max_tries attempts (each try_wait may suspend the warp for a while).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, int max_tries) {
+  for (int i = 0; i < max_tries; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+constexpr int RL_WAIT_TRIES = 1 << 20;
+
+// The parent environment of group grp into E, completing the warp's barrier
+// phase: a real environment of the previous level or, for a suffix root, the
+// real identity right environment R_{s+1} (16 bulk row copies of 128 bytes,
+// issued by lane 0), or the 1 x 1 vacuum (plain stores, then a plain arrive).
+// The caller has finished reading E (and synchronised the warp).
 __device__ __forceinline__ void stage_parent_real(const LevelParams &p, int b, const DevGroup &grp, double *E,
-                                                  int lane) {
-  if (grp.parent_slot < 0 && p.suffix) {
-    const cplx *src = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
-    for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * RL_E_STRIDE + (e & 15)] = src[e].x;
-  } else if (grp.parent_slot < 0) {
+                                                  uint64_t *bar, int lane) {
+  if (grp.parent_slot < 0 && !p.suffix) {
     for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * RL_E_STRIDE + (e & 15)] = e == 0 ? 1.0 : 0.0;
-  } else {
-    const double *src = reinterpret_cast<const double *>(p.env_prev) +
-                        ((size_t)b * p.nslot_prev + grp.parent_slot) * ENV_ELEMS;
-    for (int e = lane; e < ENV_ELEMS / 2; e += 32) cp_async16(E + (e >> 3) * RL_E_STRIDE + 2 * (e & 7), src + 2 * e);
+    __syncwarp();
+    if (lane == 0) mbar_arrive(bar);
+    return;
+  }
+  const double *src = grp.parent_slot < 0
+                          ? p.right_real + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS
+                          : reinterpret_cast<const double *>(p.env_prev) +
+                                ((size_t)b * p.nslot_prev + grp.parent_slot) * ENV_ELEMS;
+  if (lane == 0) {
+    async_proxy_fence();
+    mbar_arrive_expect_tx(bar, ENV_ELEMS * sizeof(double));
+    for (int r = 0; r < CHI; ++r) bulk_copy_g2s(E + r * RL_E_STRIDE, src + r * CHI, CHI * sizeof(double), bar);
   }
 }
 
@@ -98,28 +156,52 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
   const int first = blockIdx.x * RL_WARPS + warp;
   int count = 0;
   if (first < p.ngroups) count = min(groups_per_warp, (p.ngroups - first + stride - 1) / stride);
-  {
-    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
-    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
-    for (int e = threadIdx.x; e < SITE_ELEMS; e += RL_WARPS * 32)
-      sm.A[(e >> 5) * RL_A_STRIDE + (e & 31)] = ag[e].x;
-    for (int e = threadIdx.x; e < ENV_ELEMS; e += RL_WARPS * 32) sm.R[e] = rg[e].x;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.bar_cta, 1);
+    for (int w = 0; w < RL_WARPS; ++w) mbar_init(&sm.bar_warp[w], 1);
+    mbar_init_fence();
   }
   __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_arrive_expect_tx(&sm.bar_cta, (RL_PANEL + ENV_ELEMS) * sizeof(double));
+    bulk_copy_g2s(sm.A, p.panels + ((size_t)b * p.n + p.s) * RL_PANEL, RL_PANEL * sizeof(double), &sm.bar_cta);
+    bulk_copy_g2s(sm.R, p.right_real + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS, ENV_ELEMS * sizeof(double),
+                  &sm.bar_cta);
+  }
+  if (!mbar_wait(&sm.bar_cta, 0, RL_WAIT_TRIES)) {
+    if (threadIdx.x == 0) p.status[b] = ST_TIMEOUT;
+    mbar_wait(&sm.bar_cta, 0, RL_WAIT_TRIES);
+    return;
+  }
   const double *A = sm.A;
   const double *R = sm.R;
   double *E = sm.E[warp];
   double *S = sm.S[warp];
+  uint64_t *bar = &sm.bar_warp[warp];
+  unsigned parity = 0;
   double *env_cur = reinterpret_cast<double *>(p.env_cur);
   const int g = lane >> 2, t = lane & 3;
   if (count == 0) return;
-  stage_parent_real(p, b, p.groups[first], E, lane);
-  cp_async_commit();
+  // Group and node records are software pipelined: the next group's record is
+  // loaded while this group's first half runs (its parent slot addresses the
+  // next prefetch), and its children's node records -- at most four, one per
+  // lane, read back with shuffles -- at the end of this group. No global load
+  // of plan metadata then sits on the warp's critical path.
+  DevGroup grp = p.groups[first];
+  DevNode nd{};
+  if (lane < grp.nchild) nd = p.nodes[grp.child_begin + lane];
+  stage_parent_real(p, b, grp, E, bar, lane);
   for (int k = 0; k < count; ++k) {
     const int gidx = first + k * stride;
-    cp_async_wait<0>();
-    __syncwarp();
-    const DevGroup grp = p.groups[gidx];
+    const bool more = k + 1 < count;
+    DevGroup grp_next = grp;
+    if (more) grp_next = p.groups[gidx + stride];
+    if (!mbar_wait(bar, parity, RL_WAIT_TRIES)) {
+      if (lane == 0) p.status[b] = ST_TIMEOUT;
+      mbar_wait(bar, parity, RL_WAIT_TRIES);
+      return;
+    }
+    parity ^= 1u;
     // ---- S = Er [A_0 | A_1] (16 x 32): 32 DMMA issues
     {
       double sacc[2][4][2];
@@ -149,12 +231,11 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
             S[((col >> 4) * CHI + rt * 8 + g) * RL_S_STRIDE + (col & 15)] = sacc[rt][ct][j];
           }
     }
-    __syncwarp();   // Er is dead and S is complete: prefetch the next parent
-    if (k + 1 < count) stage_parent_real(p, b, p.groups[gidx + stride], E, lane);
-    cp_async_commit();
+    __syncwarp();   // Er is dead and S is complete: fetch the next parent
+    if (more) stage_parent_real(p, b, grp_next, E, bar, lane);
     // the parent's phase (from its first child): symmetric Er for even, antisymmetric for odd
-    const DevNode first_child = p.nodes[grp.child_begin];
-    const int kp = (first_child.phase - (first_child.code == 2 ? 1 : 0)) & 3;
+    const int c0 = __shfl_sync(0xffffffffu, nd.code, 0), k0 = __shfl_sync(0xffffffffu, nd.phase, 0);
+    const int kp = (k0 - (c0 == 2 ? 1 : 0)) & 3;
     const double sp = (kp & 1) ? -1.0 : 1.0;
     for (int cls = 0; cls < 2; ++cls) {
       if (!(grp.classes & (1 << cls))) continue;
@@ -182,7 +263,11 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
             for (int j = 0; j < 2; ++j) c[rt][ct][j] = sp * S[(ct * 8 + 2 * t + j) * RL_S_STRIDE + rt * 8 + g];
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
-        const DevNode node = p.nodes[grp.child_begin + ci];
+        DevNode node;
+        node.code = __shfl_sync(0xffffffffu, nd.code, ci);
+        node.env_slot = __shfl_sync(0xffffffffu, nd.env_slot, ci);
+        node.leaf = __shfl_sync(0xffffffffu, nd.leaf, ci);
+        node.phase = __shfl_sync(0xffffffffu, nd.phase, ci);
         const bool iz = (node.code == 0 || node.code == 3);
         if (iz != (cls == 0)) continue;
         // child symmetry: the (1,0) tile is sc times the transposed (0,1) tile
@@ -227,8 +312,9 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
       }
     }
     __syncwarp();   // S is rewritten by the next parent
+    grp = grp_next;
+    if (more && lane < grp.nchild) nd = p.nodes[grp.child_begin + lane];
   }
-  cp_async_wait<0>();
 }
 
 // The pair closures of the split evaluation on real-part environments:
@@ -256,6 +342,32 @@ split_combine_real_kernel(const double *__restrict__ left, int left_nslot, const
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   }
   if (lane == 0) leafval[(size_t)b * nleaf_total + leaf] = status[b] == 0 ? w * v : 0.0;
+}
+
+// Real site panels of one step: panel (b, s) holds the real parts of site s of
+// state b in the padded shared-memory layout of level_real_pf_kernel (row a,
+// column i * CHI + c, stride RL_A_STRIDE; padding columns zero). transposed:
+// the panel of A^T[c][i][a] = A[a][i][c] (the suffix levels).
+__global__ void __launch_bounds__(256)
+real_panels_kernel(const cplx *__restrict__ sites, int n, int transposed, double *__restrict__ panels) {
+  const size_t base = (size_t)blockIdx.y * n + blockIdx.x;
+  const cplx *a = sites + base * SITE_ELEMS;
+  double *out = panels + base * RL_PANEL;
+  for (int e = threadIdx.x; e < RL_PANEL; e += 256) {
+    const int row = e / RL_A_STRIDE, col = e - row * RL_A_STRIDE;
+    double v = 0.0;
+    if (col < 2 * CHI) {
+      const int i = col >> 4, c = col & 15;
+      v = transposed ? a[c * 2 * CHI + i * CHI + row].x : a[row * 2 * CHI + i * CHI + c].x;
+    }
+    out[e] = v;
+  }
+}
+
+// Real parts of count complex numbers.
+__global__ void __launch_bounds__(256)
+real_parts_kernel(const cplx *__restrict__ in, size_t count, double *__restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < count; i += (size_t)gridDim.x * 256) out[i] = in[i].x;
 }
 
 }  // namespace vqemps

@@ -54,6 +54,18 @@ def test_learned_proposal_beats_partition_warm_start(ws):
     assert np.median(ratios) < 1.0
 
 
+def test_time_to_same_energy_at_96_qubits(ws):
+    """The metric's target at its own size: five fixed unseen 96-qubit,
+    40,000-term Hamiltonians (the first five of the 200-instance evaluation set).
+    Every learned run reaches the plain method's final energy within 1e-4
+    relative, and the median ratio of the wall times is at most 0.5."""
+    rows, summary = ws.evaluate(WEIGHTS, count=5, seed0=900000, n=96, terms=40000)
+    assert summary["reached"] == 5 and summary["fallback"] == 0
+    for r in rows:
+        assert r["learned_best"] <= r["plain_energy"] + 1e-4 * abs(r["plain_energy"])
+    assert summary["median_ratio"] <= 0.5, [r["ratio"] for r in rows]
+
+
 def test_judgement_and_fallback(ws):
     """A proposal no better than the all-zero angles starts the refinement from
     those; a non-finite proposal falls back to the partition warm start."""
