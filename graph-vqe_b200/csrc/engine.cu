@@ -184,6 +184,9 @@ struct PartSet {
   int K = 0, n_max = 0, P_max = 0, T_max = 1, leaf_stride = 1, W = 1;
   int site_order = 0;
   bool all_diagonal = true;
+  bool real = true;                     // every partition's circuit of real gates
+  bool mixed = false;                   // some real, some complex: the per-partition chain kernels
+  int32_t *d_part_real = nullptr;       // K flags (mixed sets)
   cplx init0, init1;
   std::vector<int32_t> part_n, part_P, part_T, part_nleaf, part_idleaf, part_gate_off;
   std::vector<int> lvl_group_off, lvl_node_off, lvl_nslot;   // merged levels (n_max + 1 / n_max)
@@ -215,7 +218,7 @@ struct PartSet {
     cudaFree(d_leaf_coef); cudaFree(d_term_leaf); cudaFree(d_zmask); cudaFree(d_coeffs);
     cudaFree(d_sumidx); cudaFree(d_st_part); cudaFree(d_work);
     cudaFree(d_sched); cudaFree(d_step_off); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off);
-    cudaFree(d_part_tail_off);
+    cudaFree(d_part_tail_off); cudaFree(d_part_real);
   }
 };
 
@@ -341,6 +344,10 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   ctx->rel_cut = rel_cut;
   cudaFuncSetAttribute(evolve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(evolve_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(evolve_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(evolve_pair_real_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(evolve_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(evolve_pair_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (const char *v = std::getenv("VQEMPS_EVOLVE"))
     ctx->evolve_pair = std::strcmp(v, "chain") == 0 ? 0 : std::strcmp(v, "pair") == 0 ? 1 : -1;
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
@@ -926,9 +933,15 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
     ep.gate_q = ctx->d_gate_q;
     ep.qlist = ctx->d_qlist;
     ep.tail_off = ctx->d_tail_off;
-    evolve_pair_kernel<<<2 * B, PAIR_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+    if (ctx->real_circuit)
+      evolve_pair_real_kernel<<<2 * B, PAIR_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+    else
+      evolve_pair_kernel<<<2 * B, PAIR_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
   } else {
-    evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+    if (ctx->real_circuit)
+      evolve_real_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
+    else
+      evolve_kernel<<<B, EVOLVE_THREADS, EvolveSmem::bytes(ctx->n), st>>>(ep);
   }
   CUDA_TRY(ctx, cudaGetLastError());
   return VQEMPS_OK;

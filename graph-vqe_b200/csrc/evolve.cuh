@@ -90,6 +90,9 @@ struct EvolveParams {
   const int32_t *qlist;
   const int32_t *tail_off;
   const int32_t *part_tail_off;
+  // Mixed partition sets (the per-partition chain kernels): 1 where partition
+  // k's circuit is of real gates (real-arithmetic Jacobi), 0 where complex.
+  const int32_t *part_real;
 };
 
 constexpr int EVOLVE_THREADS = 256;   // one-CTA gate chain
@@ -453,8 +456,276 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
     return ST_OK;
 }
 
-__global__ void __launch_bounds__(EVOLVE_THREADS, 3)
-evolve_kernel(EvolveParams p) {
+// NORM[row] = sum_j X[row][j]^2 for real rows (as jacobi_row_norms).
+template <int NT>
+__device__ __forceinline__ void jacobi_row_norms_real(const double *X, double *NORM, int mr, int mc, int tid) {
+  const int grp = tid >> 4, lane = tid & 15;
+  for (int row = grp; row < mr; row += NT / 16) {
+    double a = 0.0;
+    for (int j = lane; j < mc; j += 16) a += X[row * 32 + j] * X[row * 32 + j];
+    for (int o = 8; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o, 16);
+    if (lane == 0) NORM[row] = a;
+  }
+}
+
+// The two-site update of two_site_update for a circuit of real gates: every
+// site tensor, gate and pending one-site matrix is real (imaginary parts zero),
+// so Theta, the Jacobi rotations and both factors are real and the same steps
+// run in real arithmetic: the coupling gamma = X_p . X_q is a real dot product,
+// the rotation J = c [[1, -w gamma], [w gamma, 1]] a Givens rotation (same
+// division-free formulas with |gamma|^2 = gamma^2), and each element update two
+// real multiply-adds instead of eight. The shared tiles are the complex
+// function's, used as doubles; site tensors stay complex in global memory
+// (written with zero imaginary parts). Rank rule, guard, ordering, packing
+// (including sigma_left) and the null-direction completion are the same.
+template <int NT>
+__device__ __forceinline__ int two_site_update_real(const EvolveParams &p, const EvolveShared &sh, cplx *sites_b,
+                                                    int s, int dl, int dc, int dr, cplx *us, cplx *ut,
+                                                    const cplx *gm, int *bond_next, bool sigma_left) {
+  double *X = reinterpret_cast<double *>(sh.X), *VT = reinterpret_cast<double *>(sh.VT);
+  double *SA = reinterpret_cast<double *>(sh.SA), *SB = reinterpret_cast<double *>(sh.SB);
+  double *G = reinterpret_cast<double *>(sh.G);
+  double *NORM = sh.NORM, *SIG = sh.SIG;
+  int *PERM = sh.PERM, *MISC = sh.MISC, *SCHED = sh.SCHED;
+  const int tid = threadIdx.x;
+  const double eps = 2.2204460492503131e-16;
+  const int m = 2 * dl, ncol = 2 * dr;
+  const bool tall = m > ncol;
+  const int mr = tall ? ncol : m, mc = tall ? m : ncol;
+  {
+    const cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
+    const cplx *gb = ga + SITE_ELEMS;
+    for (int e = tid; e < SITE_ELEMS; e += NT) { SA[e] = __ldcg(ga + e).x; SB[e] = __ldcg(gb + e).x; }
+    if (tid < 16) {
+      // G' = G (U_s (x) U_{s+1})
+      const int row = tid >> 2, col = tid & 3;
+      const int i = col >> 1, j = col & 1;
+      double acc = 0.0;
+      for (int ip = 0; ip < 2; ++ip)
+        for (int jp = 0; jp < 2; ++jp) acc += gm[row * 4 + ip * 2 + jp].x * (us[ip * 2 + i].x * ut[jp * 2 + j].x);
+      G[tid] = acc;
+    }
+  }
+  __syncthreads();
+  if (tid < 4) {
+    us[tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+    ut[tid] = cmake(tid == 0 || tid == 3 ? 1 : 0, 0);
+  }
+  // Theta[(l*2+I), (J*dr+r)] = sum_ij G'[(I*2+J)*4+(i*2+j)] sum_c A[l,i,c] B[c,j,r]
+  for (int lr = tid; lr < dl * dr; lr += NT) {
+    const int l = lr / dr, r = lr % dr;
+    double t00 = 0.0, t01 = 0.0, t10 = 0.0, t11 = 0.0;
+    for (int c = 0; c < dc; ++c) {
+      const double a0 = SA[(l * 2 + 0) * CHI + c], a1 = SA[(l * 2 + 1) * CHI + c];
+      const double b0 = SB[(c * 2 + 0) * CHI + r], b1 = SB[(c * 2 + 1) * CHI + r];
+      t00 = fma(a0, b0, t00); t01 = fma(a0, b1, t01); t10 = fma(a1, b0, t10); t11 = fma(a1, b1, t11);
+    }
+    for (int IJ = 0; IJ < 4; ++IJ) {
+      double v = G[IJ * 4 + 0] * t00;
+      v = fma(G[IJ * 4 + 1], t01, v);
+      v = fma(G[IJ * 4 + 2], t10, v);
+      v = fma(G[IJ * 4 + 3], t11, v);
+      const int I = IJ >> 1, J = IJ & 1;
+      if (tall) X[(J * dr + r) * 32 + (l * 2 + I)] = v;
+      else X[(l * 2 + I) * 32 + (J * dr + r)] = v;
+    }
+  }
+  for (int e = tid; e < 32 * 32; e += NT) VT[e] = (e >> 5) == (e & 31) ? 1.0 : 0.0;
+  __syncthreads();
+  jacobi_row_norms_real<NT>(X, NORM, mr, mc, tid);
+  __syncthreads();
+  double total = 0.0;
+  for (int w = 0; w < mr; ++w) total += NORM[w];
+  const double floor_g = eps * eps * total;
+  const double floor2 = floor_g * floor_g;
+  const double tol2 = 16.0 * eps * eps;
+  __syncthreads();
+  const int grp = tid >> 4, lane = tid & 15;
+  const int npairs = mr >> 1, plim = (npairs + 1) & ~1;
+  for (int e = tid; e < (mr - 1) * 16; e += NT) {
+    const int step = e >> 4, pr_ = e & 15, mm1 = mr - 1;
+    int a = 0, b = 0;
+    if (pr_ < npairs) {
+      if (pr_ == 0) { a = 0; b = 1 + (step % mm1); }
+      else { a = 1 + ((step + pr_) % mm1); b = 1 + ((step + mm1 - pr_) % mm1); }
+      if (a > b) { const int t = a; a = b; b = t; }
+    }
+    SCHED[e] = a | (b << 8);
+  }
+  __syncthreads();
+  bool converged = false;
+  for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
+    int rotated = 0;
+    for (int step = 0; step < mr - 1; ++step) {
+      for (int pair = grp; pair < plim; pair += NT / 16) {
+        const bool active = pair < npairs;
+        const int pq = SCHED[step * 16 + pair];
+        const int pr = pq & 255, qr = pq >> 8;
+        double xp0 = 0.0, xq0 = 0.0, xp1 = 0.0, xq1 = 0.0;
+        const int j0 = lane, j1 = lane + 16;
+        if (active) {
+          if (j0 < mc) { xp0 = X[pr * 32 + j0]; xq0 = X[qr * 32 + j0]; }
+          if (j1 < mc) { xp1 = X[pr * 32 + j1]; xq1 = X[qr * 32 + j1]; }
+        }
+        double gr = fma(xp1, xq1, xp0 * xq0);
+        for (int o = 8; o > 0; o >>= 1) gr += __shfl_xor_sync(0xffffffffu, gr, o, 16);
+        const double al = active ? NORM[pr] : 0.0, be = active ? NORM[qr] : 0.0;
+        const double g2 = gr * gr;
+        if (active && g2 > floor2 && g2 > tol2 * al * be) {
+          rotated = 1;
+          const double d = be - al, ad = fabs(d);
+          const double r = sqrt(d * d + 4.0 * g2);
+          const double sr = rsqrt(r * (ad + r));
+          const double wc = copysign(1.4142135623730951 * sr, d);   // w c
+          const double c = (ad + r) * sr * 0.7071067811865476;
+          const double wg2 = copysign(2.0 * g2 * r * sr * sr, d);    // w gamma^2
+          const double wg = wc * gr;                                  // w c gamma
+          if (j0 < mc) {
+            X[pr * 32 + j0] = fma(c, xp0, -wg * xq0);
+            X[qr * 32 + j0] = fma(wg, xp0, c * xq0);
+          }
+          if (j1 < mc) {
+            X[pr * 32 + j1] = fma(c, xp1, -wg * xq1);
+            X[qr * 32 + j1] = fma(wg, xp1, c * xq1);
+          }
+          for (int i = lane; i < mr; i += 16) {
+            const double vp = VT[pr * 32 + i], vq = VT[qr * 32 + i];
+            VT[pr * 32 + i] = fma(c, vp, -wg * vq);
+            VT[qr * 32 + i] = fma(wg, vp, c * vq);
+          }
+          if (lane == 0) {
+            NORM[pr] = al - wg2;
+            NORM[qr] = be + wg2;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    converged = !__syncthreads_or(rotated);
+    jacobi_row_norms_real<NT>(X, NORM, mr, mc, tid);
+    __syncthreads();
+  }
+  if (tid < mr) NORM[tid] = sqrt(NORM[tid]);
+  __syncthreads();
+  if (tid < mr) {
+    const double v = NORM[tid];
+    int rank = 0;
+    for (int q = 0; q < mr; ++q) {
+      const double w = NORM[q];
+      rank += (w > v) || (w == v && q < tid);
+    }
+    PERM[rank] = tid;
+    SIG[rank] = v;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const int r = mr;
+    int st = converged ? ST_OK : ST_NONFINITE;
+    int selected = 0;
+    const double thr = fmax(p.abs_cut, p.rel_cut * SIG[0]);
+    const bool zero_cut = (p.abs_cut == 0.0 && p.rel_cut == 0.0);
+    for (int i = 0; i < mr; ++i)
+      if (!isfinite(NORM[i])) st = ST_NONFINITE;
+    for (int i = 0; i < r; ++i)
+      if (zero_cut || SIG[i] > thr) ++selected;
+    if (st == ST_OK && zero_cut && p.max_bond < r && SIG[p.max_bond] > 64.0 * eps * r * SIG[0])
+      st = ST_INSUFFICIENT;
+    int k = selected < p.max_bond ? selected : p.max_bond;
+    if (k < 1) k = 1;
+    MISC[0] = st;
+    MISC[1] = k;
+  }
+  __syncthreads();
+  if (MISC[0] != ST_OK) return MISC[0];
+  const int k = MISC[1];
+  cplx *ga = sites_b + (size_t)s * SITE_ELEMS;
+  cplx *gb = ga + SITE_ELEMS;
+  if (tall == sigma_left) {
+    for (int e = tid; e < SITE_ELEMS; e += NT) {
+      const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
+      const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
+      double va, vb;
+      if (tall) {
+        va = (l < dl && c < k) ? X[PERM[c] * 32 + (l * 2 + I)] : 0.0;
+        vb = (cc < k && r < dr) ? VT[PERM[cc] * 32 + (J * dr + r)] : 0.0;
+      } else {
+        va = (l < dl && c < k) ? VT[PERM[c] * 32 + (l * 2 + I)] : 0.0;
+        vb = (cc < k && r < dr) ? X[PERM[cc] * 32 + (J * dr + r)] : 0.0;
+      }
+      ga[e] = cmake(va, 0.0);
+      gb[e] = cmake(vb, 0.0);
+    }
+  } else {
+    double *UC = SA;                                 // k x mc, UC[c * 32 + i]
+    const double tiny = 64.0 * eps * mr * SIG[0];
+    for (int e = tid; e < k * 32; e += NT) {
+      const int c = e >> 5, i = e & 31;
+      UC[e] = (i < mc && SIG[c] > tiny) ? X[PERM[c] * 32 + i] * (1.0 / SIG[c]) : 0.0;
+    }
+    __syncthreads();
+    if (!(SIG[k - 1] > tiny) && tid < 32) {
+      for (int c = 0; c < k; ++c) {
+        if (SIG[c] > tiny) continue;
+        for (int i0 = 0; i0 < mc; ++i0) {
+          double v = tid == i0 ? 1.0 : 0.0;
+          for (int pass = 0; pass < 2; ++pass)
+            for (int i = 0; i < c; ++i) {
+              const double u = tid < mc ? UC[i * 32 + tid] : 0.0;
+              double dt = u * v;
+              for (int o = 16; o > 0; o >>= 1) dt += __shfl_xor_sync(0xffffffffu, dt, o);
+              v -= dt * u;
+            }
+          double nn = v * v;
+          for (int o = 16; o > 0; o >>= 1) nn += __shfl_xor_sync(0xffffffffu, nn, o);
+          if (nn > 0.5 * (double)(mc - c) / mc) {
+            if (tid < mc) UC[c * 32 + tid] = v * (1.0 / sqrt(nn));
+            __syncwarp();
+            break;
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < SITE_ELEMS; e += NT) {
+      const int l = e >> 5, I = (e >> 4) & 1, c = e & 15;
+      const int cc = e >> 5, J = (e >> 4) & 1, r = e & 15;
+      double va, vb;
+      if (tall) {
+        va = (l < dl && c < k) ? UC[c * 32 + (l * 2 + I)] : 0.0;
+        vb = (cc < k && r < dr) ? VT[PERM[cc] * 32 + (J * dr + r)] * SIG[cc] : 0.0;
+      } else {
+        va = (l < dl && c < k) ? VT[PERM[c] * 32 + (l * 2 + I)] * SIG[c] : 0.0;
+        vb = (cc < k && r < dr) ? UC[cc * 32 + (J * dr + r)] : 0.0;
+      }
+      ga[e] = cmake(va, 0.0);
+      gb[e] = cmake(vb, 0.0);
+    }
+  }
+  if (tid == 0) *bond_next = k;
+  __syncthreads();
+  return ST_OK;
+}
+
+// Chain arithmetic: complex, real (a circuit of real gates), or chosen per
+// partition of a mixed partition set (EvolveParams::part_real).
+enum : int { CHAIN_COMPLEX = 0, CHAIN_REAL = 1, CHAIN_PER_PARTITION = 2 };
+
+template <int NT, int MODE>
+__device__ __forceinline__ int gate_update(const EvolveParams &p, const EvolveShared &sh, cplx *sites_b, int s,
+                                           int dl, int dc, int dr, cplx *us, cplx *ut, const cplx *gm,
+                                           int *bond_next, bool sigma_left, bool part_real) {
+  if constexpr (MODE == CHAIN_REAL) {
+    return two_site_update_real<NT>(p, sh, sites_b, s, dl, dc, dr, us, ut, gm, bond_next, sigma_left);
+  } else if constexpr (MODE == CHAIN_COMPLEX) {
+    return two_site_update<NT>(p, sh, sites_b, s, dl, dc, dr, us, ut, gm, bond_next, sigma_left);
+  } else {
+    if (part_real) return two_site_update_real<NT>(p, sh, sites_b, s, dl, dc, dr, us, ut, gm, bond_next, sigma_left);
+    return two_site_update<NT>(p, sh, sites_b, s, dl, dc, dr, us, ut, gm, bond_next, sigma_left);
+  }
+}
+
+template <int MODE>
+__device__ __forceinline__ void evolve_body(const EvolveParams &p) {
   extern __shared__ __align__(16) unsigned char smem[];
   cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
   cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
@@ -472,6 +743,7 @@ evolve_kernel(EvolveParams p) {
   const int tid = threadIdx.x;
   const int b = blockIdx.x;
   const int part = p.st_part ? p.st_part[b] : 0;
+  const bool part_real = MODE == CHAIN_PER_PARTITION && p.part_real[part] != 0;
   const int n = p.st_part ? p.part_n[part] : p.n;
   const int gate_begin = p.st_part ? p.part_gate_off[part] : 0;
   const int gate_end = p.st_part ? p.part_gate_off[part + 1] : p.ngates;
@@ -507,8 +779,9 @@ evolve_kernel(EvolveParams p) {
     }
     const int s = g.site;
     const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC, SCHED};
-    if (two_site_update<EVOLVE_THREADS>(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4, PEND + (s + 1) * 4,
-                        p.mats + g.mat, BOND + s + 1, (g.flags & GATE_SIGMA_LEFT) != 0) != ST_OK)
+    if (gate_update<EVOLVE_THREADS, MODE>(p, sh, sites_b, s, BOND[s], BOND[s + 1], BOND[s + 2], PEND + s * 4,
+                                          PEND + (s + 1) * 4, p.mats + g.mat, BOND + s + 1,
+                                          (g.flags & GATE_SIGMA_LEFT) != 0, part_real) != ST_OK)
       break;
   }
   const int status = MISC[0];
@@ -519,6 +792,18 @@ evolve_kernel(EvolveParams p) {
   for (int s = tid; s <= n; s += EVOLVE_THREADS) p.bonds[(size_t)b * (p.n + 1) + s] = BOND[s];
   if (tid == 0) p.status[b] = status;
 }
+
+__global__ void __launch_bounds__(EVOLVE_THREADS, 3)
+evolve_kernel(EvolveParams p) { evolve_body<CHAIN_COMPLEX>(p); }
+
+// The same chain for a circuit of real gates (real-arithmetic Jacobi SVD).
+__global__ void __launch_bounds__(EVOLVE_THREADS, 3)
+evolve_real_kernel(EvolveParams p) { evolve_body<CHAIN_REAL>(p); }
+
+// A partition set mixing real and complex circuits: each state's arithmetic is
+// its partition's, so every partition gets the one-partition engine's bits.
+__global__ void __launch_bounds__(EVOLVE_THREADS, 3)
+evolve_mixed_kernel(EvolveParams p) { evolve_body<CHAIN_PER_PARTITION>(p); }
 
 // 2 x 2 product of the one-site gates qlist[q0 .. q1) in program order (later
 // gates on the left).
@@ -541,8 +826,8 @@ __device__ __forceinline__ void pending_product(const EvolveParams &p, const dou
 // in global memory (read past L1 with ld.global.cg, since the other CTA writes
 // them). Both CTAs take every step, whatever the status, so the barrier counts
 // always match; after a failure the remaining gates are skipped.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
-evolve_pair_kernel(EvolveParams p) {
+template <int MODE>
+__device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem[];
@@ -562,6 +847,7 @@ evolve_pair_kernel(EvolveParams p) {
   const int rank = (int)cluster.block_rank();
   const int b = blockIdx.x >> 1;
   const int part = p.st_part ? p.st_part[b] : 0;
+  const bool part_real = MODE == CHAIN_PER_PARTITION && p.part_real[part] != 0;
   const int n = p.st_part ? p.part_n[part] : p.n;
   const double *theta_b = p.theta + (size_t)b * p.P;
   cplx *sites_b = p.sites + (size_t)b * p.n * SITE_ELEMS;
@@ -597,8 +883,8 @@ evolve_pair_kernel(EvolveParams p) {
       __syncthreads();
       const int s = g.site;
       const int dl = __ldcg(bonds_b + s), dc = __ldcg(bonds_b + s + 1), dr = __ldcg(bonds_b + s + 2);
-      const int st = two_site_update<PAIR_THREADS>(p, sh, sites_b, s, dl, dc, dr, U, U + 4, p.mats + g.mat,
-                                                   bonds_b + s + 1, (g.flags & GATE_SIGMA_LEFT) != 0);
+      const int st = gate_update<PAIR_THREADS, MODE>(p, sh, sites_b, s, dl, dc, dr, U, U + 4, p.mats + g.mat,
+                                                     bonds_b + s + 1, (g.flags & GATE_SIGMA_LEFT) != 0, part_real);
       if (st != ST_OK && tid == 0) *status_b = st;
     }
     __threadfence();
@@ -615,5 +901,16 @@ evolve_pair_kernel(EvolveParams p) {
     }
   }
 }
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
+evolve_pair_kernel(EvolveParams p) { evolve_pair_body<CHAIN_COMPLEX>(p); }
+
+// The two-CTA chain for a circuit of real gates (real-arithmetic Jacobi SVD).
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
+evolve_pair_real_kernel(EvolveParams p) { evolve_pair_body<CHAIN_REAL>(p); }
+
+// The two-CTA chain of a mixed partition set (arithmetic per partition).
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
+evolve_pair_mixed_kernel(EvolveParams p) { evolve_pair_body<CHAIN_PER_PARTITION>(p); }
 
 }  // namespace vqemps

@@ -146,7 +146,9 @@ __device__ __forceinline__ void class_tiles_real(const double *A, int xoff, cons
 
 // One trie level for B states (uniform batch: state blockIdx.y, groups
 // interleaved over the grid, groups_per_warp each), environments as real parts.
-__global__ void __launch_bounds__(RL_WARPS * 32, 4)
+// Five CTAs per SM (96 registers, 37 KB of shared memory each): measured 3 %
+// faster at 40 qubits / B = 256 than four (120 registers).
+__global__ void __launch_bounds__(RL_WARPS * 32, 5)
 level_real_pf_kernel(LevelParams p, int groups_per_warp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LevelRealSmem &sm = *reinterpret_cast<LevelRealSmem *>(smem_raw);

@@ -112,3 +112,76 @@ def test_real_levels_on_the_benchmark_batch(vq):
     for i, ref in zip(g["indices"], g["energies"]):
         assert abs(out["real_pf"][i] - ref) <= 1e-9 * max(1.0, abs(ref))
     np.testing.assert_allclose(out["real_pf"], out["dmma3_pf"], rtol=1e-11, atol=1e-9)
+
+
+@pytest.mark.parametrize("pattern", ["linear", "reverse_linear"])
+@pytest.mark.parametrize("order", ["msb", "qubit"])
+def test_real_gate_chain_state_equals_dense_state(vq, pattern, order):
+    """The real-arithmetic Jacobi chain (selected for circuits of real gates)
+    prepares the dense statevector to 1e-11, zero padding included."""
+    from oracle import mps_oracle as O
+    spec = O.hardware_efficient_spec(8, 3, ("ry",), pattern)
+    x = np.random.default_rng(3).uniform(-np.pi, np.pi, spec["count"])
+    eng = vq.Engine(0, 8)
+    eng.set_spec(spec, site_order=order)
+    ham = eng.set_hamiltonian(["Z" + "I" * 7], [1.0])
+    eng.energy(ham, x)
+    dims = eng.bond_dims()
+    raw = eng.sites(0)
+    assert np.all(raw.imag == 0.0)
+    sites = [raw[s, :dims[s], :, :dims[s + 1]] for s in range(8)]
+    if order == "msb":
+        sites = O.reverse_chain(sites)
+    np.testing.assert_allclose(O.statevector(sites), O.dense_statevector(spec, x), atol=1e-11)
+    eng.close()
+
+
+def test_real_routed_circuit_pair_equals_chain_and_dense(vq):
+    """Non-adjacent CX (SWAP routing), SWAP, H, X, Z and real U1 / U2 matrices:
+    the two-CTA and one-CTA real chains give the same bits, equal to the dense
+    state; a state with 32-row Theta blocks goes through the real Jacobi."""
+    from oracle import mps_oracle as O
+    rng = np.random.default_rng(12)
+    u = np.linalg.qr(rng.normal(size=(4, 4)))[0].astype(complex)
+    r1 = np.linalg.qr(rng.normal(size=(2, 2)))[0].astype(complex)
+    ops = [("h", 0), ("ry", 1, 0), ("cx", 0, 4), ("u2", 2, 5, u), ("ry", 4, 1), ("cx", 5, 3), ("swap", 1, 6),
+           ("u1", 3, r1), ("cx", 6, 2), ("z", 0), ("x", 6), ("ry", 6, 2), ("cx", 1, 2), ("h", 3), ("cx", 0, 5),
+           ("ry", 3, 3, 0.5)]
+    x = rng.uniform(-np.pi, np.pi, 4)
+    words = ["".join(rng.choice(list("IXYZ"), 7)) for _ in range(50)]
+    coeffs = rng.normal(size=50)
+    out = {}
+    for mode in ("pair", "chain"):
+        eng = vq.Engine(0, 16)
+        eng.set_evolve_mode(mode)
+        eng.set_level_variant("real_pf")
+        eng.set_circuit(7, ops, site_order="msb")
+        ham = eng.set_hamiltonian(words, coeffs)
+        e, pt = eng.energy(ham, x, per_term=True)
+        out[mode] = (e.cpu().numpy(), pt.cpu().numpy(), eng.sites(0), eng.bond_dims())
+        eng.close()
+    assert np.array_equal(out["pair"][2], out["chain"][2]) and out["pair"][3] == out["chain"][3]
+    assert np.array_equal(out["pair"][0], out["chain"][0])
+    # the dense reference: U1 / U2 through their matrices
+    psi = np.zeros(2 ** 7, dtype=complex)
+    psi[0] = 1.0
+    psi = psi.reshape([2] * 7)
+    for op in ops:
+        if op[0] == "cx" or op[0] == "swap" or op[0] == "u2":
+            a, b = op[1], op[2]
+            m = {"cx": np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=complex),
+                 "swap": np.array([[1, 0, 0, 0], [0, 0, 1, 0], [0, 1, 0, 0], [0, 0, 0, 1]], dtype=complex),
+                 "u2": op[3] if op[0] == "u2" else None}[op[0]]
+            t = np.tensordot(m.reshape(2, 2, 2, 2), psi, axes=([2, 3], [a, b]))
+            psi = np.moveaxis(t, [0, 1], [a, b])
+        else:
+            if op[0] == "u1":
+                m = op[2]
+            elif op[0] == "ry":
+                ang = x[op[2]] * (op[3] if len(op) > 3 else 1.0)
+                m = O.rotation("ry", ang)
+            else:
+                m = O.FIXED_MATRICES[op[0]]
+            psi = np.moveaxis(np.tensordot(m, psi, axes=([1], [op[1]])), 0, op[1])
+    dense = O.dense_expectations(psi.reshape(-1), words).real
+    np.testing.assert_allclose(out["pair"][1][0], dense, atol=1e-11)
