@@ -280,6 +280,7 @@ struct vqemps_ctx {
   DevBuf<int32_t> bonds_ws, status;
   DevBuf<double> leafval, theta_stage, energy_stage, per_term_stage;
   DevBuf<double> panels, panels_t, right_real;   // real-arithmetic levels: real site panels, real R
+  bool right_real_fresh = false;        // right_real holds the last launch_right's environments
   DevBuf<uint64_t> bits, seeds;
   DevBuf<int32_t> zsum;
   DevBuf<cplx> branch;
@@ -952,9 +953,19 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
 static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st, cplx *branch) {
   const int nleaf = h ? std::max(h->e_nleaf(), 1) : 0;
   if (h) CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
-  right_env_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
-                                               ctx->status.ptr, h ? ctx->leafval.ptr : nullptr,
-                                               nleaf, h ? h->e_identity_leaf() : -1);
+  if (ctx->real_circuit) {
+    // real arithmetic, and the real copy the real-arithmetic levels stage
+    CUDA_TRY(ctx, ctx->right_real.ensure((size_t)B * (ctx->n + 1) * ENV_ELEMS));
+    right_env_real_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
+                                                      ctx->status.ptr, h ? ctx->leafval.ptr : nullptr, nleaf,
+                                                      h ? h->e_identity_leaf() : -1, ctx->right_real.ptr);
+    ctx->right_real_fresh = true;
+  } else {
+    right_env_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
+                                                 ctx->status.ptr, h ? ctx->leafval.ptr : nullptr,
+                                                 nleaf, h ? h->e_identity_leaf() : -1);
+    ctx->right_real_fresh = false;
+  }
   CUDA_TRY(ctx, cudaGetLastError());
   return VQEMPS_OK;
 }
@@ -1029,10 +1040,12 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 1, ctx->panels_t.ptr);
       CUDA_TRY(ctx, cudaGetLastError());
     }
-    const size_t rcount = (size_t)B * (n + 1) * ENV_ELEMS;
-    real_parts_kernel<<<(unsigned)std::min<size_t>((rcount + 255) / 256, 4096), 256, 0, st>>>(ctx->right.ptr, rcount,
-                                                                                           ctx->right_real.ptr);
-    CUDA_TRY(ctx, cudaGetLastError());
+    if (!ctx->right_real_fresh) {       // launch_right wrote only the complex environments
+      const size_t rcount = (size_t)B * (n + 1) * ENV_ELEMS;
+      real_parts_kernel<<<(unsigned)std::min<size_t>((rcount + 255) / 256, 4096), 256, 0, st>>>(
+          ctx->right.ptr, rcount, ctx->right_real.ptr);
+      CUDA_TRY(ctx, cudaGetLastError());
+    }
   }
   if (split) {
     // suffix levels n-1 .. cut on transposed site tensors, starting from R_{l+1}

@@ -366,6 +366,71 @@ real_panels_kernel(const cplx *__restrict__ sites, int n, int transposed, double
   }
 }
 
+// Identity right environments of states with real amplitudes (right_env_kernel
+// in real arithmetic): R_n = 1, R_s[b][b'] = sum_{i,c,c'} A[b][i][c] R_{s+1}[c][c']
+// A[b'][i][c'] with A real, one CTA per state. The outputs are those of
+// right_env_kernel -- R and the branch matrices M_i as complex numbers with zero
+// imaginary parts, the norm in the identity leaf -- plus the real parts of every
+// R_s in right_real, the copy the real-arithmetic levels stage. The site tile is
+// padded to 33 doubles per row, so the first contraction's 16 rows of a
+// half-warp fall on distinct banks.
+__global__ void __launch_bounds__(RIGHT_THREADS)
+right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right,
+                      cplx *__restrict__ branch, const int32_t *__restrict__ status,
+                      double *__restrict__ leafval, int nleaf_total, int identity_leaf,
+                      double *__restrict__ right_real) {
+  constexpr int AS = 2 * CHI + 1;
+  __shared__ double A[CHI * AS];
+  __shared__ double R[ENV_ELEMS];
+  __shared__ double T[2 * ENV_ELEMS];
+  const int b = blockIdx.x, tid = threadIdx.x;
+  const cplx *sb = sites + (size_t)b * n * SITE_ELEMS;
+  cplx *rb = right + (size_t)b * (n + 1) * ENV_ELEMS;
+  double *rr = right_real + (size_t)b * (n + 1) * ENV_ELEMS;
+  cplx *mbase = branch ? branch + (size_t)b * n * 2 * ENV_ELEMS : nullptr;
+  R[tid] = tid == 0 ? 1.0 : 0.0;
+  rb[(size_t)n * ENV_ELEMS + tid] = cmake(R[tid], 0.0);
+  rr[(size_t)n * ENV_ELEMS + tid] = R[tid];
+  for (int s = n - 1; s >= 0; --s) {
+    for (int e = tid; e < SITE_ELEMS; e += RIGHT_THREADS) A[(e >> 5) * AS + (e & 31)] = sb[(size_t)s * SITE_ELEMS + e].x;
+    __syncthreads();
+    // T_i[c][b'] = sum_c' R[c][c'] A[b'][i][c']
+    {
+      const int c = tid >> 4, bp = tid & 15;
+      double t0 = 0.0, t1 = 0.0;
+      for (int cp = 0; cp < CHI; ++cp) {
+        const double r = R[c * CHI + cp];
+        t0 = fma(r, A[bp * AS + cp], t0);
+        t1 = fma(r, A[bp * AS + CHI + cp], t1);
+      }
+      T[c * CHI + bp] = t0;
+      T[ENV_ELEMS + c * CHI + bp] = t1;
+    }
+    __syncthreads();
+    // R_s[bb][b'] = sum_i M_i[bb][b'],  M_i[bb][b'] = sum_c A[bb][i][c] T_i[c][b']
+    {
+      const int bb = tid >> 4, bp = tid & 15;
+      double m0 = 0.0, m1 = 0.0;
+      for (int c = 0; c < CHI; ++c) {
+        m0 = fma(A[bb * AS + c], T[c * CHI + bp], m0);
+        m1 = fma(A[bb * AS + CHI + c], T[ENV_ELEMS + c * CHI + bp], m1);
+      }
+      const double acc = m0 + m1;
+      R[tid] = acc;
+      rb[(size_t)s * ENV_ELEMS + tid] = cmake(acc, 0.0);
+      rr[(size_t)s * ENV_ELEMS + tid] = acc;
+      if (mbase != nullptr) {
+        cplx *mb = mbase + (size_t)s * 2 * ENV_ELEMS;
+        mb[tid] = cmake(m0, 0.0);
+        mb[ENV_ELEMS + tid] = cmake(m1, 0.0);
+      }
+    }
+    __syncthreads();
+  }
+  if (identity_leaf >= 0 && leafval != nullptr && tid == 0)
+    leafval[(size_t)b * nleaf_total + identity_leaf] = status[b] == 0 ? R[0] : 0.0;
+}
+
 // Real parts of count complex numbers.
 __global__ void __launch_bounds__(256)
 real_parts_kernel(const cplx *__restrict__ in, size_t count, double *__restrict__ out) {
