@@ -49,15 +49,17 @@ constexpr int RIGHT_THREADS = 256;
 
 __device__ __forceinline__ void right_env_body(const cplx *__restrict__ sb, int n, cplx *__restrict__ rb,
                                                cplx *__restrict__ mbase, bool ok, double *leafslot) {
-  __shared__ cplx A[SITE_ELEMS];
+  // site tile rows padded to 33 elements: the first contraction's 16 rows of a
+  // half-warp then fall on distinct banks
+  constexpr int AS = 2 * CHI + 1;
+  __shared__ cplx A[CHI * AS];
   __shared__ cplx R[ENV_ELEMS];
   __shared__ cplx T[2 * ENV_ELEMS];
   const int tid = threadIdx.x;
   R[tid] = cmake(tid == 0 ? 1.0 : 0.0, 0.0);
   rb[(size_t)n * ENV_ELEMS + tid] = R[tid];
   for (int s = n - 1; s >= 0; --s) {
-    A[tid] = sb[(size_t)s * SITE_ELEMS + tid];
-    A[tid + 256] = sb[(size_t)s * SITE_ELEMS + tid + 256];
+    for (int e = tid; e < SITE_ELEMS; e += RIGHT_THREADS) A[(e >> 5) * AS + (e & 31)] = sb[(size_t)s * SITE_ELEMS + e];
     __syncthreads();
     // T_i[c, b'] = sum_c' R[c,c'] A[b',i,c']
     {
@@ -65,8 +67,8 @@ __device__ __forceinline__ void right_env_body(const cplx *__restrict__ sb, int 
       cplx t0 = cmake(0, 0), t1 = cmake(0, 0);
       for (int cp = 0; cp < CHI; ++cp) {
         const cplx r = R[c * CHI + cp];
-        cfma(t0, r, A[(bp * 2 + 0) * CHI + cp]);
-        cfma(t1, r, A[(bp * 2 + 1) * CHI + cp]);
+        cfma(t0, r, A[bp * AS + cp]);
+        cfma(t1, r, A[bp * AS + CHI + cp]);
       }
       T[c * CHI + bp] = t0;
       T[ENV_ELEMS + c * CHI + bp] = t1;
@@ -77,8 +79,8 @@ __device__ __forceinline__ void right_env_body(const cplx *__restrict__ sb, int 
       const int bb = tid >> 4, bp = tid & 15;
       cplx m0 = cmake(0, 0), m1 = cmake(0, 0);
       for (int c = 0; c < CHI; ++c) {
-        cfma_conj(m0, A[(bb * 2 + 0) * CHI + c], T[c * CHI + bp]);
-        cfma_conj(m1, A[(bb * 2 + 1) * CHI + c], T[ENV_ELEMS + c * CHI + bp]);
+        cfma_conj(m0, A[bb * AS + c], T[c * CHI + bp]);
+        cfma_conj(m1, A[bb * AS + CHI + c], T[ENV_ELEMS + c * CHI + bp]);
       }
       const cplx acc = cadd(m0, m1);
       R[tid] = acc;

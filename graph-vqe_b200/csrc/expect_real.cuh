@@ -18,19 +18,22 @@
 // three (Gauss): 56 DMMA issues per one-class parent instead of 168, and the
 // environments moved between levels are half the bytes.
 //
-// Shared tiles hold doubles, padded so that the fragment loads of a half-warp
-// (lanes g = 0..3 rows, t = 0..3 columns) fall on 16 distinct 8-byte banks:
-// row strides are 4 mod 16 doubles.
+// Shared tiles hold doubles laid out so that the fragment loads of a half-warp
+// (lanes g = 0..3 rows, t = 0..3 columns) fall on 16 distinct 8-byte banks: the
+// site panel and S pad their rows to 4 mod 16 doubles; environments keep 16
+// doubles per row with the 4-column blocks of row r XOR-swizzled by r mod 4
+// (rl_swz), in global memory as well as in shared memory, so the swizzle costs
+// no bytes and an environment moves as one contiguous 2,048-byte block.
 //
 // Tile movement is by the bulk-copy (TMA) engine: real_panels_kernel writes every
 // site tensor once per step as a real panel already in the padded shared-memory
 // layout, so a CTA stages its site panel and right environment with two 1-D
 // cp.async.bulk copies (4,608 + 2,048 bytes), and each warp fetches the next
-// parent environment with 16 row copies of 128 bytes into its padded tile; all
-// complete on mbarriers (expect_tx), one per CTA and one per warp. Sources are
-// this GPU's memory, addresses 16-byte aligned, sizes multiples of 16, and no
-// copy uses cluster multicast. Every wait is bounded: a wait that gives up marks
-// the state ST_TIMEOUT, waits once more (bounded) for its copies and returns.
+// parent environment with one 2,048-byte copy; all complete on mbarriers
+// (expect_tx), one per CTA and one per warp. Sources are this GPU's memory,
+// addresses 16-byte aligned, sizes multiples of 16, and no copy uses cluster
+// multicast. Every wait is bounded: a wait that gives up marks the state
+// ST_TIMEOUT, waits once more (bounded) for its copies and returns.
 #pragma once
 #include "common.cuh"
 #include "expect.cuh"
@@ -39,16 +42,20 @@
 namespace vqemps {
 
 constexpr int RL_WARPS = 4;
-constexpr int RL_E_STRIDE = 20;   // E: 16 rows of 16 doubles
 constexpr int RL_A_STRIDE = 36;   // site panel: 16 rows [a] of 32 doubles [i * 16 + c]
 constexpr int RL_S_STRIDE = 20;   // S = Er [A_0 | A_1]: [i][a][c], 2 x 16 rows of 16 doubles
 
 constexpr int RL_PANEL = CHI * RL_A_STRIDE;   // doubles per real site panel (4,608 bytes)
 
+// Position of element (r, c) of a real environment (16 x 16, row-major) in the
+// swizzled layout: column blocks of four XORed with r mod 4. Two-element runs
+// (c even) stay contiguous and 16-byte aligned.
+__host__ __device__ __forceinline__ int rl_swz(int r, int c) { return r * CHI + (c ^ ((r & 3) << 2)); }
+
 struct LevelRealSmem {
   double A[RL_PANEL];
-  double R[ENV_ELEMS];
-  double E[RL_WARPS][CHI * RL_E_STRIDE];
+  double R[ENV_ELEMS];             // swizzled (rl_swz)
+  double E[RL_WARPS][ENV_ELEMS];   // swizzled (rl_swz)
   double S[RL_WARPS][2 * CHI * RL_S_STRIDE];
   uint64_t bar_cta;                 // site panel + right environment
   uint64_t bar_warp[RL_WARPS];      // each warp's parent environment
@@ -96,13 +103,14 @@ constexpr int RL_WAIT_TRIES = 1 << 20;
 
 // The parent environment of group grp into E, completing the warp's barrier
 // phase: a real environment of the previous level or, for a suffix root, the
-// real identity right environment R_{s+1} (16 bulk row copies of 128 bytes,
-// issued by lane 0), or the 1 x 1 vacuum (plain stores, then a plain arrive).
+// real identity right environment R_{s+1} (one 2,048-byte bulk copy issued by
+// lane 0; both are stored swizzled), or the 1 x 1 vacuum (plain stores, then a
+// plain arrive; element (0, 0) sits at position 0 in either layout).
 // The caller has finished reading E (and synchronised the warp).
 __device__ __forceinline__ void stage_parent_real(const LevelParams &p, int b, const DevGroup &grp, double *E,
                                                   uint64_t *bar, int lane) {
   if (grp.parent_slot < 0 && !p.suffix) {
-    for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * RL_E_STRIDE + (e & 15)] = e == 0 ? 1.0 : 0.0;
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[e] = e == 0 ? 1.0 : 0.0;
     __syncwarp();
     if (lane == 0) mbar_arrive(bar);
     return;
@@ -114,7 +122,7 @@ __device__ __forceinline__ void stage_parent_real(const LevelParams &p, int b, c
   if (lane == 0) {
     async_proxy_fence();
     mbar_arrive_expect_tx(bar, ENV_ELEMS * sizeof(double));
-    for (int r = 0; r < CHI; ++r) bulk_copy_g2s(E + r * RL_E_STRIDE, src + r * CHI, CHI * sizeof(double), bar);
+    bulk_copy_g2s(E, src, ENV_ELEMS * sizeof(double), bar);
   }
 }
 
@@ -146,7 +154,7 @@ __device__ __forceinline__ void class_tiles_real(const double *A, int xoff, cons
 
 // One trie level for B states (uniform batch: state blockIdx.y, groups
 // interleaved over the grid, groups_per_warp each), environments as real parts.
-// Five CTAs per SM (96 registers, 37 KB of shared memory each): measured 3 %
+// Five CTAs per SM (96 registers, 35 KB of shared memory each): measured 3 %
 // faster at 40 qubits / B = 256 than four (120 registers).
 __global__ void __launch_bounds__(RL_WARPS * 32, 5)
 level_real_pf_kernel(LevelParams p, int groups_per_warp) {
@@ -215,7 +223,7 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
       for (int ks = 0; ks < 4; ++ks) {
         double ef[2], pf[4];
 #pragma unroll
-        for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * RL_E_STRIDE + ks * 4 + t];
+        for (int rt = 0; rt < 2; ++rt) ef[rt] = E[rl_swz(rt * 8 + g, ks * 4 + t)];
 #pragma unroll
         for (int ct = 0; ct < 4; ++ct) pf[ct] = A[(ks * 4 + t) * RL_A_STRIDE + ct * 8 + g];
 #pragma unroll
@@ -290,10 +298,10 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
           for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
             for (int ct = rt; ct < 2; ++ct)
+              *reinterpret_cast<double2 *>(dst + rl_swz(rt * 8 + g, ct * 8 + 2 * t)) =
+                  make_double2(out[rt][ct][0], out[rt][ct][1]);
 #pragma unroll
-              for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
-#pragma unroll
-          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = sc * out[0][1][j];
+          for (int j = 0; j < 2; ++j) dst[rl_swz(8 + 2 * t + j, g)] = sc * out[0][1][j];
         }
         if (node.leaf >= 0) {
           const double w = re_ipow(node.phase);
@@ -304,9 +312,9 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
 #pragma unroll
               for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
-                for (int j = 0; j < 2; ++j) v += out[rt][ct][j] * R[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j];
+                for (int j = 0; j < 2; ++j) v += out[rt][ct][j] * R[rl_swz(rt * 8 + g, ct * 8 + 2 * t + j)];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) v += sc * out[0][1][j] * R[(8 + 2 * t + j) * CHI + g];
+            for (int j = 0; j < 2; ++j) v += sc * out[0][1][j] * R[rl_swz(8 + 2 * t + j, g)];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
           }
           if (lane == 0) p.leafval[(size_t)b * p.nleaf_total + node.leaf] = w * v;
@@ -321,6 +329,7 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
 
 // The pair closures of the split evaluation on real-part environments:
 // value = Re(i^(prefix phase + suffix phase)) sum_xy L[x][y] R[x][y] (pair_sign).
+// Both sides are stored swizzled alike, so the elementwise sum reads them flat.
 __global__ void __launch_bounds__(COMBINE_WARPS * 32)
 split_combine_real_kernel(const double *__restrict__ left, int left_nslot, const double *__restrict__ right,
                           int right_nslot, const int32_t *__restrict__ pairs, const double *__restrict__ pair_sign,
@@ -371,7 +380,8 @@ real_panels_kernel(const cplx *__restrict__ sites, int n, int transposed, double
 // A[b'][i][c'] with A real, one CTA per state. The outputs are those of
 // right_env_kernel -- R and the branch matrices M_i as complex numbers with zero
 // imaginary parts, the norm in the identity leaf -- plus the real parts of every
-// R_s in right_real, the copy the real-arithmetic levels stage. The site tile is
+// R_s in right_real (swizzled, rl_swz), the copy the real-arithmetic levels
+// stage. The site tile is
 // padded to 33 doubles per row, so the first contraction's 16 rows of a
 // half-warp fall on distinct banks.
 __global__ void __launch_bounds__(RIGHT_THREADS)
@@ -390,7 +400,7 @@ right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ 
   cplx *mbase = branch ? branch + (size_t)b * n * 2 * ENV_ELEMS : nullptr;
   R[tid] = tid == 0 ? 1.0 : 0.0;
   rb[(size_t)n * ENV_ELEMS + tid] = cmake(R[tid], 0.0);
-  rr[(size_t)n * ENV_ELEMS + tid] = R[tid];
+  rr[(size_t)n * ENV_ELEMS + rl_swz(tid >> 4, tid & 15)] = R[tid];
   for (int s = n - 1; s >= 0; --s) {
     for (int e = tid; e < SITE_ELEMS; e += RIGHT_THREADS) A[(e >> 5) * AS + (e & 31)] = sb[(size_t)s * SITE_ELEMS + e].x;
     __syncthreads();
@@ -418,7 +428,7 @@ right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ 
       const double acc = m0 + m1;
       R[tid] = acc;
       rb[(size_t)s * ENV_ELEMS + tid] = cmake(acc, 0.0);
-      rr[(size_t)s * ENV_ELEMS + tid] = acc;
+      rr[(size_t)s * ENV_ELEMS + rl_swz(bb, bp)] = acc;
       if (mbase != nullptr) {
         cplx *mb = mbase + (size_t)s * 2 * ENV_ELEMS;
         mb[tid] = cmake(m0, 0.0);
@@ -431,10 +441,13 @@ right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ 
     leafval[(size_t)b * nleaf_total + identity_leaf] = status[b] == 0 ? R[0] : 0.0;
 }
 
-// Real parts of count complex numbers.
+// Real parts of count / ENV_ELEMS complex environments, each stored swizzled (rl_swz).
 __global__ void __launch_bounds__(256)
 real_parts_kernel(const cplx *__restrict__ in, size_t count, double *__restrict__ out) {
-  for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < count; i += (size_t)gridDim.x * 256) out[i] = in[i].x;
+  for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < count; i += (size_t)gridDim.x * 256) {
+    const int e = (int)(i % ENV_ELEMS);
+    out[i - e + rl_swz(e >> 4, e & 15)] = in[i].x;
+  }
 }
 
 }  // namespace vqemps
