@@ -306,8 +306,7 @@ def main():
               "dmma3_pf": "level_mma3_pf_kernel (FP64 DMMA tensor cores, Gauss 3-product complex multiply, "
                           "cp.async parent prefetch)",
               "real_pf": "level_real_pf_kernel (FP64 DMMA tensor cores, real arithmetic with Y-count phases for "
-                         "real-amplitude states, cp.async parent prefetch)"}.get(variant,
-                                                                                                    str(variant))
+                         "real-amplitude states, 1-D bulk-copy staging on mbarriers)"}.get(variant, str(variant))
     traffic = profiled_traffic(variant)
     roofline = dict(bound="tensor" if variant and variant != "simt" and variant != "simt_pf" else "fp64",
                     achieved=achieved,
@@ -357,8 +356,8 @@ def main():
                                 l2="working set per step > L2 (env buffers ~4 GB): no flush needed",
                                 plain_evals_per_s=plain_rate, batched_over_plain=value / world / plain_rate,
                                 flops_per_eval=flops_eval, survey_flops_per_eval=stats["flops_survey"],
-                                trie_node_sites=stats["node_sites"], phases_ms=phases["ms"],
-                                golden_gate=gate),
+                                trie_node_sites=stats["node_sites"],
+                                phases_ms=phases["ms"], golden_gate=gate),
                     roofline=roofline, cpu_baseline=cpu, e2e=e2e,
                     gpu_launches=phases["launches_per_step"] * args.steps,
                     clocks=clock_info)

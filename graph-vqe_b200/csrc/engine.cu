@@ -97,14 +97,45 @@ struct Hamiltonian {
   // slot); those of suffix slot r are pr_idx[pr_off[r] .. pr_off[r+1]-1].
   std::vector<int32_t> pl_off, pr_off, pr_idx;
   int32_t *d_pl_off = nullptr, *d_pr_off = nullptr, *d_pr_idx = nullptr;
+  // Per-term cuts (energies; multicut_plan.inc): every word closes at its own
+  // cut c_t, the prefix levels run 0..c_t-1 and the suffix levels c_t..l_t of it.
+  // Levels keep their environments in per-level regions of one buffer per half
+  // (region of level s: B x stride[s] slots from B x base[s]), since closures
+  // read them at many levels. The gradient keeps the single-cut plan.
+  bool mcut = false;                     // the current call uses the per-term-cut plan (select_plan)
+  bool mc_pending = false, mc_built = false;
+  // inputs kept for the deferred build: suffix-trie node of word t at site s
+  // (n x T), suffix nodes per site, last sites, bond dims at load time
+  std::vector<int32_t> mc_rslot, mc_sid_count;
+  std::vector<int> mc_last, mc_bd;
+  std::vector<int> mp_group_off, mp_node_off, mp_stride, mp_base;   // prefix levels 0 .. mp_levels - 1
+  std::vector<DevGroup> mp_groups;
+  std::vector<DevNode> mp_nodes;
+  std::vector<int> ms_group_off, ms_node_off, ms_stride, ms_base;   // suffix levels, by site (n + 1 / n)
+  std::vector<DevGroup> ms_groups;
+  std::vector<DevNode> ms_nodes;
+  std::vector<DevPair> mc_pairs;
+  std::vector<double> mc_pair_sign, mc_leaf_coef;
+  std::vector<int32_t> mc_term_leaf;
+  int mp_levels = 0, ms_low = 0, mc_nleaf = 0, mc_identity_leaf = -1, mc_npairs = 0;
+  long long mp_slots = 0, ms_slots = 0, mc_node_sites = 0, mc_groups_total = 0;
+  int mc_max_slot = 1;
+  double mc_flops = 0.0;
+  std::vector<int32_t> term_node;        // n x T: term t's prefix-trie node at level s (kept for the deferred build)
+  DevGroup *d_mp_groups = nullptr, *d_ms_groups = nullptr;
+  DevNode *d_mp_nodes = nullptr, *d_ms_nodes = nullptr;
+  DevPair *d_mc_pairs = nullptr;
+  double *d_mc_pair_sign = nullptr, *d_mc_leaf_coef = nullptr;
+  int32_t *d_mc_term_leaf = nullptr;
+  unsigned char *d_arena_mc = nullptr;   // the per-term-cut plan's device arrays
   // every d_ array above is a slice of this one device allocation
   unsigned char *d_arena = nullptr;
-  ~Hamiltonian() { cudaFree(d_arena); }
+  ~Hamiltonian() { cudaFree(d_arena); cudaFree(d_arena_mc); }
   // leaves of the energy path (split plan when cut >= 0)
-  int e_nleaf() const { return cut >= 0 ? split_nleaf : nleaf; }
-  int e_identity_leaf() const { return cut >= 0 ? split_identity_leaf : identity_leaf; }
-  const double *e_leaf_coef() const { return cut >= 0 ? d_split_leaf_coef : d_leaf_coef; }
-  const int32_t *e_term_leaf() const { return cut >= 0 ? d_split_term_leaf : d_term_leaf; }
+  int e_nleaf() const { return mcut ? mc_nleaf : cut >= 0 ? split_nleaf : nleaf; }
+  int e_identity_leaf() const { return mcut ? mc_identity_leaf : cut >= 0 ? split_identity_leaf : identity_leaf; }
+  const double *e_leaf_coef() const { return mcut ? d_mc_leaf_coef : cut >= 0 ? d_split_leaf_coef : d_leaf_coef; }
+  const int32_t *e_term_leaf() const { return mcut ? d_mc_term_leaf : cut >= 0 ? d_split_term_leaf : d_term_leaf; }
 };
 
 // As-soon-as-possible schedule of a circuit's two-site gates for the two-CTA gate
@@ -281,6 +312,14 @@ struct vqemps_ctx {
   DevBuf<double> leafval, theta_stage, energy_stage, per_term_stage;
   DevBuf<double> panels, panels_t, right_real;   // real-arithmetic levels: real site panels, real R
   bool right_real_fresh = false;        // right_real holds the last launch_right's environments
+  bool panels_fresh = false;            // ... and panels (panels_t too when panels_t_fresh) its site panels
+  bool panels_t_fresh = false;
+  DevBuf<cplx> mflat_p, mflat_s;        // per-term-cut plan: level regions of the prefix / suffix half
+  int level_launches = 0;               // kernels the last run_levels launched
+  // The split evaluation's suffix half runs on a second stream, forked from and
+  // joined back into the caller's stream (so graph capture sees both).
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   DevBuf<uint64_t> bits, seeds;
   DevBuf<int32_t> zsum;
   DevBuf<cplx> branch;
@@ -306,6 +345,9 @@ struct vqemps_ctx {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
     cudaFree(d_sched); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
   }
 };
 
@@ -629,6 +671,7 @@ extern "C" int vqemps_bond_dims(const vqemps_ctx *ctx, int *dims) {
   return VQEMPS_OK;
 }
 
+#include "multicut_plan.inc"
 #include "split_plan.inc"
 
 // ---------------------------------------------------------------------------
@@ -713,6 +756,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   h->node_off.assign(n + 1, 0);
   h->nslot.assign(n, 0);
   h->term_slot.assign((size_t)n * T, -1);   // level-major: one level's writes stay in one row
+  h->term_node.assign((size_t)n * T, -1);
   h->level_flops.assign(n, 0.0);
   const std::vector<int> &bd = ctx->bonds;
   for (int s = 0; s < n; ++s) {
@@ -762,7 +806,10 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         h->nodes[h->node_off[s] + k].env_slot = slot_of[k];
       }
     h->nslot[s] = slots;
-    for (size_t j = 0; j < active.size(); ++j) h->term_slot[(size_t)s * T + active[j]] = slot_of[node_of[j]];
+    for (size_t j = 0; j < active.size(); ++j) {
+      h->term_slot[(size_t)s * T + active[j]] = slot_of[node_of[j]];
+      h->term_node[(size_t)s * T + active[j]] = node_of[j];
+    }
     h->max_slot = std::max(h->max_slot, slots);
     // groups: consecutive nodes with the same parent
     {
@@ -806,6 +853,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   h->node_off[n] = (int)h->nodes.size();
   build_split_plan(*h, code, last, ctx->bonds, ctx->split_mode);
   std::vector<int32_t>().swap(h->term_slot);
+  if (!h->mc_pending) std::vector<int32_t>().swap(h->term_node);
   // upload: every plan array is a 256-byte aligned slice of ONE device
   // allocation, filled by one copy of a packed host image (tens of separate
   // allocations and copies cost more than the plan build itself at 40,000 terms)
@@ -861,6 +909,68 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   return VQEMPS_OK;
 }
 
+// Batches of at least this many states evaluate energies with the per-term-cut
+// plan (multicut_plan.inc); smaller ones with the single cut, so callers that
+// evaluate a Hamiltonian a few states at a time never pay for the build.
+constexpr int MC_MIN_BATCH = 32;
+
+// Build and upload the per-term-cut plan once (one device allocation), then
+// release its inputs.
+static int ensure_multicut(vqemps_ctx *ctx, Hamiltonian *h) {
+  if (!h->mc_pending) return VQEMPS_OK;
+  h->mc_pending = false;
+  CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+  build_multicut_plan(*h);
+  std::vector<int32_t>().swap(h->term_node);
+  std::vector<int32_t>().swap(h->mc_rslot);
+  std::vector<int32_t>().swap(h->mc_sid_count);
+  if (!h->mc_built) return VQEMPS_OK;
+  struct Slice {
+    void **dst;
+    const void *src;
+    size_t bytes, off;
+  };
+  std::vector<Slice> slices;
+  size_t total = 0;
+  auto add = [&](auto *&dst, const auto &vec) {
+    using E = typename std::remove_reference<decltype(vec)>::type::value_type;
+    const size_t bytes = vec.size() * sizeof(E);
+    slices.push_back({reinterpret_cast<void **>(&dst), vec.data(), bytes, total});
+    total += (std::max<size_t>(bytes, sizeof(E)) + 255) & ~(size_t)255;
+  };
+  add(h->d_mp_groups, h->mp_groups);
+  add(h->d_mp_nodes, h->mp_nodes);
+  add(h->d_ms_groups, h->ms_groups);
+  add(h->d_ms_nodes, h->ms_nodes);
+  add(h->d_mc_pairs, h->mc_pairs);
+  add(h->d_mc_pair_sign, h->mc_pair_sign);
+  add(h->d_mc_leaf_coef, h->mc_leaf_coef);
+  add(h->d_mc_term_leaf, h->mc_term_leaf);
+  std::vector<unsigned char> image(total, 0);
+  for (const Slice &sl : slices)
+    if (sl.bytes) std::memcpy(image.data() + sl.off, sl.src, sl.bytes);
+  const cudaError_t e = cudaMalloc(&h->d_arena_mc, std::max<size_t>(total, 256));
+  if (e != cudaSuccess) {
+    h->mc_built = false;
+    h->d_arena_mc = nullptr;
+    return fail(ctx, VQEMPS_CUDA_ERROR, std::string("per-term-cut plan upload: ") + cudaGetErrorString(e));
+  }
+  for (const Slice &sl : slices) *sl.dst = h->d_arena_mc + sl.off;
+  CUDA_TRY(ctx, cudaMemcpy(h->d_arena_mc, image.data(), total, cudaMemcpyHostToDevice));
+  return VQEMPS_OK;
+}
+
+// The energy path's plan for this call (B states): sets h->mcut, which the leaf
+// accessors and run_levels follow.
+static int select_plan(vqemps_ctx *ctx, Hamiltonian *h, int B) {
+  h->mcut = false;
+  if (h->cut < 0 || B < MC_MIN_BATCH) return VQEMPS_OK;
+  const int rc = ensure_multicut(ctx, h);
+  if (rc) return rc;
+  h->mcut = h->mc_built;
+  return VQEMPS_OK;
+}
+
 extern "C" int vqemps_free_hamiltonian(vqemps_ctx *ctx, int handle) {
   if (!ctx) return VQEMPS_INVALID;
   cudaSetDevice(ctx->device);
@@ -875,18 +985,23 @@ extern "C" int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stat
   if (!ctx || !stats) return VQEMPS_INVALID;
   auto it = ctx->hams.find(handle);
   if (it == ctx->hams.end()) return VQEMPS_INVALID;
-  const Hamiltonian &h = *it->second;
+  Hamiltonian &h = *it->second;
+  // the plan of a large batch: the per-term-cut plan where it applies
+  const int rc = ensure_multicut(const_cast<vqemps_ctx *>(ctx), &h);
+  if (rc) return rc;
+  const bool mc = h.mc_built;
   const bool split = h.cut >= 0;
-  stats[0] = split ? h.split_flops : h.flops;
+  stats[0] = mc ? h.mc_flops : split ? h.split_flops : h.flops;
   stats[1] = h.flops_survey;
-  stats[2] = split ? (double)h.split_node_sites : (double)h.node_sites;
-  stats[3] = split ? (double)(h.sl_groups.size() + h.sr_groups.size()) : (double)h.groups.size();
-  stats[4] = (double)h.e_nleaf();
-  stats[5] = split ? (double)std::max(h.sl_max_slot, h.sr_max_slot) : (double)h.max_slot;
+  stats[2] = mc ? (double)h.mc_node_sites : split ? (double)h.split_node_sites : (double)h.node_sites;
+  stats[3] = mc ? (double)h.mc_groups_total
+                : split ? (double)(h.sl_groups.size() + h.sr_groups.size()) : (double)h.groups.size();
+  stats[4] = (double)(mc ? h.mc_nleaf : split ? h.split_nleaf : h.nleaf);
+  stats[5] = mc ? (double)h.mc_max_slot : split ? (double)std::max(h.sl_max_slot, h.sr_max_slot) : (double)h.max_slot;
   stats[6] = (double)h.cut;
   stats[7] = h.flops;
   stats[8] = (double)h.node_sites;
-  stats[9] = (double)h.npairs;
+  stats[9] = (double)(mc ? h.mc_npairs : h.npairs);
   return VQEMPS_OK;
 }
 
@@ -954,17 +1069,25 @@ static int launch_right(vqemps_ctx *ctx, Hamiltonian *h, int B, cudaStream_t st,
   const int nleaf = h ? std::max(h->e_nleaf(), 1) : 0;
   if (h) CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
   if (ctx->real_circuit) {
-    // real arithmetic, and the real copy the real-arithmetic levels stage
+    // real arithmetic, and the real copies the real-arithmetic levels stage: R,
+    // the site panels and, for a split plan, the transposed panels
+    const bool panels = h != nullptr, panels_t = h != nullptr && h->cut >= 0;
     CUDA_TRY(ctx, ctx->right_real.ensure((size_t)B * (ctx->n + 1) * ENV_ELEMS));
+    if (panels) CUDA_TRY(ctx, ctx->panels.ensure((size_t)B * ctx->n * RL_PANEL));
+    if (panels_t) CUDA_TRY(ctx, ctx->panels_t.ensure((size_t)B * ctx->n * RL_PANEL));
     right_env_real_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
                                                       ctx->status.ptr, h ? ctx->leafval.ptr : nullptr, nleaf,
-                                                      h ? h->e_identity_leaf() : -1, ctx->right_real.ptr);
+                                                      h ? h->e_identity_leaf() : -1, ctx->right_real.ptr,
+                                                      panels ? ctx->panels.ptr : nullptr,
+                                                      panels_t ? ctx->panels_t.ptr : nullptr);
     ctx->right_real_fresh = true;
+    ctx->panels_fresh = panels;
+    ctx->panels_t_fresh = panels_t;
   } else {
     right_env_kernel<<<B, RIGHT_THREADS, 0, st>>>(ctx->sites.ptr, ctx->n, ctx->right.ptr, branch,
                                                  ctx->status.ptr, h ? ctx->leafval.ptr : nullptr,
                                                  nleaf, h ? h->e_identity_leaf() : -1);
-    ctx->right_real_fresh = false;
+    ctx->right_real_fresh = ctx->panels_fresh = ctx->panels_t_fresh = false;
   }
   CUDA_TRY(ctx, cudaGetLastError());
   return VQEMPS_OK;
@@ -1021,37 +1144,179 @@ static void launch_level_variant(int variant, const LevelParams &lp, int ng, int
 }
 
 // All trie levels of one evaluation with a given variant (needs launch_right first).
+// Inputs of the real-arithmetic levels that launch_right did not write: real
+// site panels (and transposed ones for suffix levels) and the real parts of R.
+static int prepare_real_inputs(vqemps_ctx *ctx, int B, bool transposed, cudaStream_t st) {
+  const int n = ctx->n;
+  int &nl = ctx->level_launches;
+  CUDA_TRY(ctx, ctx->panels.ensure((size_t)B * n * RL_PANEL));
+  CUDA_TRY(ctx, ctx->right_real.ensure((size_t)B * (n + 1) * ENV_ELEMS));
+  if (!(ctx->right_real_fresh && ctx->panels_fresh)) {
+    real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 0, ctx->panels.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  if (transposed && !(ctx->right_real_fresh && ctx->panels_t_fresh)) {
+    CUDA_TRY(ctx, ctx->panels_t.ensure((size_t)B * n * RL_PANEL));
+    real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 1, ctx->panels_t.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  if (!ctx->right_real_fresh) {       // launch_right wrote only the complex environments
+    const size_t rcount = (size_t)B * (n + 1) * ENV_ELEMS;
+    real_parts_kernel<<<(unsigned)std::min<size_t>((rcount + 255) / 256, 4096), 256, 0, st>>>(
+        ctx->right.ptr, rcount, ctx->right_real.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  return VQEMPS_OK;
+}
+
+// Fork the split evaluation's suffix half onto the second stream: returns the
+// stream to launch it on (joined back by join_suffix before the pair closures).
+static int fork_suffix(vqemps_ctx *ctx, cudaStream_t st, cudaStream_t *sst) {
+  if (!ctx->aux) {
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&ctx->aux, cudaStreamNonBlocking));
+    CUDA_TRY(ctx, cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(ctx, cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming));
+  }
+  CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, st));
+  CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->aux, ctx->ev_fork, 0));
+  *sst = ctx->aux;
+  return VQEMPS_OK;
+}
+static int join_suffix(vqemps_ctx *ctx, cudaStream_t st, cudaStream_t sst) {
+  CUDA_TRY(ctx, cudaEventRecord(ctx->ev_join, sst));
+  CUDA_TRY(ctx, cudaStreamWaitEvent(st, ctx->ev_join, 0));
+  return VQEMPS_OK;
+}
+
+// All trie levels of one evaluation with the per-term-cut plan (h.mcut): the
+// suffix levels (second stream) and the prefix levels write their environments
+// into per-level regions of mflat_s / mflat_p, then the pair closures.
+static int run_levels_mcut(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int variant) {
+  const int n = ctx->n;
+  const int nleaf = std::max(h.e_nleaf(), 1);
+  const bool real = variant == LV_REALPF4;
+  int &nl = ctx->level_launches;
+  nl = 0;
+  if (real) {
+    const int rc = prepare_real_inputs(ctx, B, true, st);
+    if (rc) return rc;
+  }
+  // a region's first element: real environments are ENV_ELEMS doubles, complex ones ENV_ELEMS cplx
+  const size_t unit = real ? 1 : 2;
+  auto region = [&](DevBuf<cplx> &f, int base) {
+    return reinterpret_cast<cplx *>(reinterpret_cast<double *>(f.ptr) + (size_t)B * base * ENV_ELEMS * unit);
+  };
+  cudaStream_t sst = st;
+  {
+    const int rc = fork_suffix(ctx, st, &sst);
+    if (rc) return rc;
+  }
+  if (!real) {
+    transpose_sites_kernel<<<dim3(n, B), 256, 0, sst>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  for (int s = n - 1; s >= h.ms_low; --s) {
+    const int ng = h.ms_group_off[s + 1] - h.ms_group_off[s];
+    if (ng == 0) continue;                        // sites beyond every suffix path
+    LevelParams lp{};
+    lp.sites = ctx->sites_t.ptr;
+    lp.right = ctx->right.ptr;
+    lp.env_prev = region(ctx->mflat_s, s + 1 < n ? h.ms_base[s + 1] : 0);
+    lp.env_cur = region(ctx->mflat_s, h.ms_base[s]);
+    lp.groups = h.d_ms_groups + h.ms_group_off[s];
+    lp.nodes = h.d_ms_nodes + h.ms_node_off[s];
+    lp.leafval = ctx->leafval.ptr;
+    lp.ngroups = ng;
+    lp.nslot_prev = s + 1 < n ? h.ms_stride[s + 1] : 1;
+    lp.nslot_cur = h.ms_stride[s];
+    lp.nleaf_total = nleaf;
+    lp.n = n;
+    lp.s = s;
+    lp.suffix = 1;
+    lp.panels = ctx->panels_t.ptr;
+    lp.right_real = ctx->right_real.ptr;
+    lp.status = ctx->status.ptr;
+    launch_level_variant(variant == LV_MMA3PF4 || variant == LV_REALPF4 ? variant : LV_MMAPF4, lp, ng, B,
+                         ctx->sm_count, sst);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  for (int s = 0; s < h.mp_levels; ++s) {
+    const int ng = h.mp_group_off[s + 1] - h.mp_group_off[s];
+    if (ng == 0) continue;
+    LevelParams lp{};
+    lp.sites = ctx->sites.ptr;
+    lp.right = ctx->right.ptr;
+    lp.env_prev = region(ctx->mflat_p, s > 0 ? h.mp_base[s - 1] : 0);
+    lp.env_cur = region(ctx->mflat_p, h.mp_base[s]);
+    lp.groups = h.d_mp_groups + h.mp_group_off[s];
+    lp.nodes = h.d_mp_nodes + h.mp_node_off[s];
+    lp.leafval = ctx->leafval.ptr;
+    lp.ngroups = ng;
+    lp.nslot_prev = s > 0 ? h.mp_stride[s - 1] : 1;
+    lp.nslot_cur = h.mp_stride[s];
+    lp.nleaf_total = nleaf;
+    lp.n = n;
+    lp.s = s;
+    lp.panels = ctx->panels.ptr;
+    lp.right_real = ctx->right_real.ptr;
+    lp.status = ctx->status.ptr;
+    launch_level_variant(variant, lp, ng, B, ctx->sm_count, st);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  {
+    const int rc = join_suffix(ctx, st, sst);
+    if (rc) return rc;
+  }
+  if (h.mc_npairs > 0) {
+    const dim3 grid((h.mc_npairs + COMBINE_WARPS - 1) / COMBINE_WARPS, B);
+    if (real)
+      pair_combine_real_kernel<<<grid, COMBINE_WARPS * 32, 0, st>>>(
+          reinterpret_cast<const double *>(ctx->mflat_p.ptr), reinterpret_cast<const double *>(ctx->mflat_s.ptr),
+          h.d_mc_pairs, h.d_mc_pair_sign, h.mc_npairs, ctx->status.ptr, ctx->leafval.ptr, nleaf);
+    else
+      pair_combine_kernel<<<grid, COMBINE_WARPS * 32, 0, st>>>(ctx->mflat_p.ptr, ctx->mflat_s.ptr, h.d_mc_pairs,
+                                                               h.mc_npairs, ctx->status.ptr, ctx->leafval.ptr,
+                                                               nleaf);
+    CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  return VQEMPS_OK;
+}
+
 static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, int variant) {
   if (variant == LV_REALPF4 && !ctx->real_circuit)
     return fail(ctx, VQEMPS_INVALID, "the real-arithmetic level kernels need a circuit of real gates");
+  if (h.mcut) return run_levels_mcut(ctx, h, B, st, variant);
   const int n = ctx->n;
   const int nleaf = std::max(h.e_nleaf(), 1);
   const bool split = h.cut >= 0;
   const int top = split ? h.cut : n;                // prefix levels run on sites 0 .. top - 1
   const bool real = variant == LV_REALPF4;
+  int &nl = ctx->level_launches;
+  nl = 0;
   if (real) {
-    // real site panels (and transposed ones for the suffix levels) and real R
-    CUDA_TRY(ctx, ctx->panels.ensure((size_t)B * n * RL_PANEL));
-    CUDA_TRY(ctx, ctx->right_real.ensure((size_t)B * (n + 1) * ENV_ELEMS));
-    real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 0, ctx->panels.ptr);
-    CUDA_TRY(ctx, cudaGetLastError());
-    if (split) {
-      CUDA_TRY(ctx, ctx->panels_t.ensure((size_t)B * n * RL_PANEL));
-      real_panels_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, 1, ctx->panels_t.ptr);
-      CUDA_TRY(ctx, cudaGetLastError());
-    }
-    if (!ctx->right_real_fresh) {       // launch_right wrote only the complex environments
-      const size_t rcount = (size_t)B * (n + 1) * ENV_ELEMS;
-      real_parts_kernel<<<(unsigned)std::min<size_t>((rcount + 255) / 256, 4096), 256, 0, st>>>(
-          ctx->right.ptr, rcount, ctx->right_real.ptr);
-      CUDA_TRY(ctx, cudaGetLastError());
-    }
+    const int rc2 = prepare_real_inputs(ctx, B, split, st);
+    if (rc2) return rc2;
+  }
+  // the suffix half (stream sst) and the prefix half are independent until the
+  // pair closures: fork the suffix half onto the second stream
+  cudaStream_t sst = st;
+  if (split) {
+    const int rc2 = fork_suffix(ctx, st, &sst);
+    if (rc2) return rc2;
   }
   if (split) {
     // suffix levels n-1 .. cut on transposed site tensors, starting from R_{l+1}
     if (!real) {
-      transpose_sites_kernel<<<dim3(n, B), 256, 0, st>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
+      transpose_sites_kernel<<<dim3(n, B), 256, 0, sst>>>(ctx->sites.ptr, n, ctx->sites_t.ptr);
       CUDA_TRY(ctx, cudaGetLastError());
+      ++nl;
     }
     cplx *renv[2] = {ctx->env2.ptr, ctx->env3.ptr};
     for (int s = n - 1; s >= h.cut; --s) {
@@ -1076,8 +1341,9 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       lp.right_real = ctx->right_real.ptr;
       lp.status = ctx->status.ptr;
       launch_level_variant(variant == LV_MMA3PF4 || variant == LV_REALPF4 ? variant : LV_MMAPF4, lp, ng, B,
-                           ctx->sm_count, st);
+                           ctx->sm_count, sst);
       CUDA_TRY(ctx, cudaGetLastError());
+      ++nl;
     }
   }
   cplx *envs[2] = {ctx->env0.ptr, ctx->env1.ptr};
@@ -1103,6 +1369,11 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.status = ctx->status.ptr;
     launch_level_variant(variant, lp, ng, B, ctx->sm_count, st);
     CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
+  }
+  if (split) {   // join the suffix half
+    const int rc2 = join_suffix(ctx, st, sst);
+    if (rc2) return rc2;
   }
   if (split && h.npairs > 0) {
     const dim3 grid((h.npairs + COMBINE_WARPS - 1) / COMBINE_WARPS, B);
@@ -1117,6 +1388,7 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
           left, std::max(h.nslot[h.cut - 1], 1), right, std::max(h.sr_nslot[h.cut], 1), h.d_pairs, h.npairs,
           ctx->status.ptr, ctx->leafval.ptr, nleaf);
     CUDA_TRY(ctx, cudaGetLastError());
+    ++nl;
   }
   return VQEMPS_OK;
 }
@@ -1191,13 +1463,20 @@ static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st
                          double *energies_dev, double *per_term_dev) {
   const int nleaf = std::max(h.e_nleaf(), 1);
   CUDA_TRY(ctx, ctx->leafval.ensure((size_t)B * nleaf));
-  const size_t pre_slots = h.cut >= 0 ? h.sl_max_slot : h.max_slot;
-  CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * pre_slots * ENV_ELEMS));
-  CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * pre_slots * ENV_ELEMS));
-  if (h.cut >= 0) {
-    CUDA_TRY(ctx, ctx->env2.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
-    CUDA_TRY(ctx, ctx->env3.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
+  if (h.mcut) {
+    // every level keeps its environments (complex size; the real levels use half)
+    CUDA_TRY(ctx, ctx->mflat_p.ensure((size_t)B * h.mp_slots * ENV_ELEMS));
+    CUDA_TRY(ctx, ctx->mflat_s.ensure((size_t)B * h.ms_slots * ENV_ELEMS));
     CUDA_TRY(ctx, ctx->sites_t.ensure((size_t)B * ctx->n * SITE_ELEMS));
+  } else {
+    const size_t pre_slots = h.cut >= 0 ? h.sl_max_slot : h.max_slot;
+    CUDA_TRY(ctx, ctx->env0.ensure((size_t)B * pre_slots * ENV_ELEMS));
+    CUDA_TRY(ctx, ctx->env1.ensure((size_t)B * pre_slots * ENV_ELEMS));
+    if (h.cut >= 0) {
+      CUDA_TRY(ctx, ctx->env2.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
+      CUDA_TRY(ctx, ctx->env3.ensure((size_t)B * h.sr_max_slot * ENV_ELEMS));
+      CUDA_TRY(ctx, ctx->sites_t.ensure((size_t)B * ctx->n * SITE_ELEMS));
+    }
   }
   int variant = LV_SIMT4;
   int rc = pick_variant(ctx, h, B, st, &variant);
@@ -1261,7 +1540,9 @@ extern "C" int vqemps_energy_batch(vqemps_ctx *ctx, int handle, const double *th
     return fail(ctx, VQEMPS_INVALID, "bad batch arguments");
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = as_stream(stream);
-  int rc = ensure_state_ws(ctx, B);
+  int rc = select_plan(ctx, h, B);
+  if (rc) return rc;
+  rc = ensure_state_ws(ctx, B);
   if (rc) return rc;
   rc = launch_evolve(ctx, theta_dev, B, st);
   if (rc) return rc;
@@ -1283,7 +1564,9 @@ extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *
   if (!h || B < 1) return fail(ctx, VQEMPS_INVALID, "bad profile arguments");
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   cudaStream_t st = as_stream(stream);
-  int rc = ensure_state_ws(ctx, B);
+  int rc = select_plan(ctx, h, B);
+  if (rc) return rc;
+  rc = ensure_state_ws(ctx, B);
   if (rc) return rc;
   CUDA_TRY(ctx, ctx->energy_stage.ensure((size_t)B));
   cudaEvent_t ev[5];
@@ -1312,16 +1595,7 @@ extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *
   ms[1] = t[1];
   ms[3] = t[3];
   ms[2] = t[2] - t[3];   // launch_levels includes one reduction
-  int nlev = 0;
-  const int top = h->cut >= 0 ? h->cut : ctx->n;
-  for (int s = 0; s < top; ++s)
-    if (h->group_off[s + 1] > h->group_off[s]) ++nlev;
-  if (h->cut >= 0) {
-    nlev += 1 + (h->npairs > 0 ? 1 : 0);            // transpose + pair closures
-    for (int s = h->cut; s < ctx->n; ++s)
-      if (h->sr_group_off[s + 1] > h->sr_group_off[s]) ++nlev;
-  }
-  *launches = 1 + 1 + nlev + 1;
+  *launches = 1 + 1 + ctx->level_launches + 1;   // gate chain, right environments, levels, reduction
   for (auto &e : ev) cudaEventDestroy(e);
   ctx->last_B = B;
   return VQEMPS_OK;

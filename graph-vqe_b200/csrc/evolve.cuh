@@ -277,10 +277,15 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
       SCHED[e] = a | (b << 8);
     }
     __syncthreads();
+    // Converged once mr - 1 consecutive steps rotate nothing: such a window
+    // visits every pair exactly once (across a sweep boundary too), each with no
+    // rotation since -- half a sweep earlier on average than waiting for a whole
+    // quiet sweep.
     bool converged = false;
+    int quiet = 0;
     for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
-      int rotated = 0;
       for (int step = 0; step < mr - 1; ++step) {
+        int rotated = 0;
         // pairs grp, grp + NT/16, ... of the step (one pass when NT = 256); the
         // pairs of a step touch disjoint rows, so their order does not matter.
         // The bound is even, so both 16-lane groups of a warp take the same
@@ -334,9 +339,12 @@ __device__ __forceinline__ int two_site_update(const EvolveParams &p, const Evol
             }
           }
         }
-        __syncthreads();
+        quiet = __syncthreads_or(rotated) ? 0 : quiet + 1;
+        if (quiet >= mr - 1) {
+          converged = true;
+          break;
+        }
       }
-      converged = !__syncthreads_or(rotated);
       jacobi_row_norms<NT>(X, NORM, mr, mc, tid);
       __syncthreads();
     }
@@ -554,9 +562,10 @@ __device__ __forceinline__ int two_site_update_real(const EvolveParams &p, const
   }
   __syncthreads();
   bool converged = false;
+  int quiet = 0;   // consecutive steps without a rotation (see two_site_update)
   for (int sweep = 0; sweep < JACOBI_MAX_SWEEPS && !converged; ++sweep) {
-    int rotated = 0;
     for (int step = 0; step < mr - 1; ++step) {
+      int rotated = 0;
       for (int pair = grp; pair < plim; pair += NT / 16) {
         const bool active = pair < npairs;
         const int pq = SCHED[step * 16 + pair];
@@ -599,9 +608,12 @@ __device__ __forceinline__ int two_site_update_real(const EvolveParams &p, const
           }
         }
       }
-      __syncthreads();
+      quiet = __syncthreads_or(rotated) ? 0 : quiet + 1;
+      if (quiet >= mr - 1) {
+        converged = true;
+        break;
+      }
     }
-    converged = !__syncthreads_or(rotated);
     jacobi_row_norms_real<NT>(X, NORM, mr, mc, tid);
     __syncthreads();
   }

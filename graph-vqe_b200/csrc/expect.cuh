@@ -515,6 +515,38 @@ transpose_sites_kernel(const cplx *__restrict__ in, int n, cplx *__restrict__ ou
 // Pair closures of the split evaluation: leafval[b][leaf] = Re sum L o R for
 // (prefix slot, suffix slot, leaf) triples; one warp per pair.
 constexpr int COMBINE_WARPS = 8;
+
+// A pair closure of the per-term-cut plan: its two operands by region (the level
+// region of B x nslot slots starting at slot B x base of its half's buffer) and slot.
+struct DevPair {
+  int32_t lbase, lnslot, lslot;
+  int32_t rbase, rnslot, rslot;
+  int32_t leaf, pad;
+};
+__device__ __forceinline__ size_t pair_offset(int base, int nslot, int slot, int b, int B) {
+  return ((size_t)B * base + (size_t)b * nslot + slot) * ENV_ELEMS;
+}
+
+// Pair closures of the per-term-cut plan (complex environments).
+__global__ void __launch_bounds__(COMBINE_WARPS * 32)
+pair_combine_kernel(const cplx *__restrict__ left, const cplx *__restrict__ right, const DevPair *__restrict__ pairs,
+                    int npairs, const int32_t *__restrict__ status, double *__restrict__ leafval,
+                    int nleaf_total) {
+  const int b = blockIdx.y, B = gridDim.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pidx = blockIdx.x * COMBINE_WARPS + warp;
+  if (pidx >= npairs) return;
+  const DevPair pr = pairs[pidx];
+  const cplx *L = left + pair_offset(pr.lbase, pr.lnslot, pr.lslot, b, B);
+  const cplx *R = right + pair_offset(pr.rbase, pr.rnslot, pr.rslot, b, B);
+  double v = 0.0;
+  for (int e = lane; e < ENV_ELEMS; e += 32) {
+    const cplx l = L[e], r = R[e];
+    v += l.x * r.x - l.y * r.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) leafval[(size_t)b * nleaf_total + pr.leaf] = status[b] == 0 ? v : 0.0;
+}
 __global__ void __launch_bounds__(COMBINE_WARPS * 32)
 split_combine_kernel(const cplx *__restrict__ left, int left_nslot, const cplx *__restrict__ right,
                      int right_nslot, const int32_t *__restrict__ pairs, int npairs,

@@ -126,11 +126,9 @@ __device__ __forceinline__ void stage_parent_real(const LevelParams &p, int b, c
   }
 }
 
-// acc = A_x^T S_y over the 8 x 8 output tiles (rt, ct) (x = column offset 0 or
-// CHI of the site panel, y = panel half); SKIP10 leaves the (1,0) tile out.
-template <bool SKIP10>
-__device__ __forceinline__ void class_tiles_real(const double *A, int xoff, const double *S, int y,
-                                                 double (&acc)[2][2][2], int g, int t) {
+// The X/Y class product t0 = A_0^T S_1 over all four 8 x 8 output tiles.
+__device__ __forceinline__ void class_tiles_real_xy(const double *A, const double *S, double (&acc)[2][2][2],
+                                                    int g, int t) {
 #pragma unroll
   for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
@@ -139,15 +137,44 @@ __device__ __forceinline__ void class_tiles_real(const double *A, int xoff, cons
   for (int ks = 0; ks < 4; ++ks) {
     double x[2], yv[2];
 #pragma unroll
-    for (int rt = 0; rt < 2; ++rt) x[rt] = A[(ks * 4 + t) * RL_A_STRIDE + xoff + rt * 8 + g];
+    for (int rt = 0; rt < 2; ++rt) x[rt] = A[(ks * 4 + t) * RL_A_STRIDE + rt * 8 + g];
 #pragma unroll
-    for (int ct = 0; ct < 2; ++ct) yv[ct] = S[(y * CHI + ks * 4 + t) * RL_S_STRIDE + ct * 8 + g];
+    for (int ct = 0; ct < 2; ++ct) yv[ct] = S[(CHI + ks * 4 + t) * RL_S_STRIDE + ct * 8 + g];
 #pragma unroll
     for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-      for (int ct = 0; ct < 2; ++ct) {
-        if (SKIP10 && rt == 1 && ct == 0) continue;
-        dmma(acc[rt][ct][0], acc[rt][ct][1], x[rt], yv[ct]);
+      for (int ct = 0; ct < 2; ++ct) dmma(acc[rt][ct][0], acc[rt][ct][1], x[rt], yv[ct]);
+  }
+}
+
+// The I/Z class pair in one pass: a = A_0^T S_0 and c = A_1^T S_1 over the
+// tiles (0,0), (0,1), (1,1) -- six independent accumulators per k-step, so
+// consecutive DMMA issues of a warp do not wait on each other.
+__device__ __forceinline__ void class_tiles_real_iz(const double *A, const double *S, double (&a)[2][2][2],
+                                                    double (&c)[2][2][2], int g, int t) {
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct) a[rt][ct][0] = a[rt][ct][1] = c[rt][ct][0] = c[rt][ct][1] = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks) {
+    double x0[2], x1[2], y0[2], y1[2];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt) {
+      x0[rt] = A[(ks * 4 + t) * RL_A_STRIDE + rt * 8 + g];
+      x1[rt] = A[(ks * 4 + t) * RL_A_STRIDE + CHI + rt * 8 + g];
+    }
+#pragma unroll
+    for (int ct = 0; ct < 2; ++ct) {
+      y0[ct] = S[(ks * 4 + t) * RL_S_STRIDE + ct * 8 + g];
+      y1[ct] = S[(CHI + ks * 4 + t) * RL_S_STRIDE + ct * 8 + g];
+    }
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = rt; ct < 2; ++ct) {
+        dmma(a[rt][ct][0], a[rt][ct][1], x0[rt], y0[ct]);
+        dmma(c[rt][ct][0], c[rt][ct][1], x1[rt], y1[ct]);
       }
   }
 }
@@ -253,10 +280,9 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
       // X/Y: t0 = A_0^T S_1 (four tiles), t1 = A_1^T S_0 = sp t0^T through the panel
       double a[2][2][2], c[2][2][2];
       if (cls == 0) {
-        class_tiles_real<true>(A, 0, S, 0, a, g, t);
-        class_tiles_real<true>(A, CHI, S, 1, c, g, t);
+        class_tiles_real_iz(A, S, a, c, g, t);
       } else {
-        class_tiles_real<false>(A, 0, S, 1, a, g, t);
+        class_tiles_real_xy(A, S, a, g, t);
         __syncwarp();   // the panel is consumed: t0 goes into its place
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
@@ -329,7 +355,38 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
 
 // The pair closures of the split evaluation on real-part environments:
 // value = Re(i^(prefix phase + suffix phase)) sum_xy L[x][y] R[x][y] (pair_sign).
-// Both sides are stored swizzled alike, so the elementwise sum reads them flat.
+// A pair with a nonzero sign has an even phase sum, so L and R are both
+// symmetric or both antisymmetric and L[y][x] R[y][x] = L[x][y] R[x][y]: the sum
+// is the diagonal plus twice the upper triangle. A warp reads only the 4-column
+// blocks that reach the diagonal or above -- 40 of the 64 blocks of 32 bytes
+// (both sides are stored swizzled alike, rl_swz) -- 5/8 of the bytes.
+__device__ __forceinline__ double real_pair_dot(const double *L, const double *R, int lane) {
+  double v = 0.0;
+  // block q of the upper part: rows 0-3 four blocks each, rows 4-7 three (from
+  // block 1), rows 8-11 two (from 2), rows 12-15 one (block 3)
+  for (int q = lane; q < 40; q += 32) {
+    int r, lb;
+    if (q < 16) { r = q >> 2; lb = q & 3; }
+    else if (q < 28) { r = 4 + (q - 16) / 3; lb = 1 + (q - 16) % 3; }
+    else if (q < 36) { r = 8 + ((q - 28) >> 1); lb = 2 + ((q - 28) & 1); }
+    else { r = 12 + (q - 36); lb = 3; }
+    const int off = rl_swz(r, 4 * lb);
+    const double2 l0 = *reinterpret_cast<const double2 *>(L + off);
+    const double2 l1 = *reinterpret_cast<const double2 *>(L + off + 2);
+    const double2 r0 = *reinterpret_cast<const double2 *>(R + off);
+    const double2 r1 = *reinterpret_cast<const double2 *>(R + off + 2);
+    const double lv[4] = {l0.x, l0.y, l1.x, l1.y}, rv[4] = {r0.x, r0.y, r1.x, r1.y};
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = 4 * lb + j;
+      const double wt = c > r ? 2.0 : (c == r ? 1.0 : 0.0);
+      v = fma(wt * lv[j], rv[j], v);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __global__ void __launch_bounds__(COMBINE_WARPS * 32)
 split_combine_real_kernel(const double *__restrict__ left, int left_nslot, const double *__restrict__ right,
                           int right_nslot, const int32_t *__restrict__ pairs, const double *__restrict__ pair_sign,
@@ -342,17 +399,28 @@ split_combine_real_kernel(const double *__restrict__ left, int left_nslot, const
   const int ls = pairs[3 * pidx], rs = pairs[3 * pidx + 1], leaf = pairs[3 * pidx + 2];
   const double w = pair_sign[pidx];
   double v = 0.0;
-  if (w != 0.0) {
-    const double2 *L = reinterpret_cast<const double2 *>(left + ((size_t)b * left_nslot + ls) * ENV_ELEMS);
-    const double2 *R = reinterpret_cast<const double2 *>(right + ((size_t)b * right_nslot + rs) * ENV_ELEMS);
-    for (int e = lane; e < ENV_ELEMS / 2; e += 32) {
-      const double2 l = L[e], r = R[e];
-      v = fma(l.x, r.x, v);
-      v = fma(l.y, r.y, v);
-    }
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  }
+  if (w != 0.0)
+    v = real_pair_dot(left + ((size_t)b * left_nslot + ls) * ENV_ELEMS,
+                      right + ((size_t)b * right_nslot + rs) * ENV_ELEMS, lane);
   if (lane == 0) leafval[(size_t)b * nleaf_total + leaf] = status[b] == 0 ? w * v : 0.0;
+}
+
+// The same closures for the per-term-cut plan (operands by level region).
+__global__ void __launch_bounds__(COMBINE_WARPS * 32)
+pair_combine_real_kernel(const double *__restrict__ left, const double *__restrict__ right,
+                         const DevPair *__restrict__ pairs, const double *__restrict__ pair_sign, int npairs,
+                         const int32_t *__restrict__ status, double *__restrict__ leafval, int nleaf_total) {
+  const int b = blockIdx.y, B = gridDim.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pidx = blockIdx.x * COMBINE_WARPS + warp;
+  if (pidx >= npairs) return;
+  const DevPair pr = pairs[pidx];
+  const double w = pair_sign[pidx];
+  double v = 0.0;
+  if (w != 0.0)
+    v = real_pair_dot(left + pair_offset(pr.lbase, pr.lnslot, pr.lslot, b, B),
+                      right + pair_offset(pr.rbase, pr.rnslot, pr.rslot, b, B), lane);
+  if (lane == 0) leafval[(size_t)b * nleaf_total + pr.leaf] = status[b] == 0 ? w * v : 0.0;
 }
 
 // Real site panels of one step: panel (b, s) holds the real parts of site s of
@@ -381,14 +449,17 @@ real_panels_kernel(const cplx *__restrict__ sites, int n, int transposed, double
 // right_env_kernel -- R and the branch matrices M_i as complex numbers with zero
 // imaginary parts, the norm in the identity leaf -- plus the real parts of every
 // R_s in right_real (swizzled, rl_swz), the copy the real-arithmetic levels
-// stage. The site tile is
+// stage, and -- when panels / panels_t are non-null -- every site's real panel
+// and transposed panel (real_panels_kernel's output) from the staged tile, so
+// the levels need no separate panel pass. The site tile is
 // padded to 33 doubles per row, so the first contraction's 16 rows of a
 // half-warp fall on distinct banks.
 __global__ void __launch_bounds__(RIGHT_THREADS)
 right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ right,
                       cplx *__restrict__ branch, const int32_t *__restrict__ status,
                       double *__restrict__ leafval, int nleaf_total, int identity_leaf,
-                      double *__restrict__ right_real) {
+                      double *__restrict__ right_real, double *__restrict__ panels,
+                      double *__restrict__ panels_t) {
   constexpr int AS = 2 * CHI + 1;
   __shared__ double A[CHI * AS];
   __shared__ double R[ENV_ELEMS];
@@ -404,6 +475,17 @@ right_env_real_kernel(const cplx *__restrict__ sites, int n, cplx *__restrict__ 
   for (int s = n - 1; s >= 0; --s) {
     for (int e = tid; e < SITE_ELEMS; e += RIGHT_THREADS) A[(e >> 5) * AS + (e & 31)] = sb[(size_t)s * SITE_ELEMS + e].x;
     __syncthreads();
+    if (panels != nullptr) {
+      // panel row a, column i * CHI + c: A[a][i][c]; transposed: row c, column i * CHI + a
+      double *pn = panels + ((size_t)b * n + s) * RL_PANEL;
+      double *pt = panels_t != nullptr ? panels_t + ((size_t)b * n + s) * RL_PANEL : nullptr;
+      for (int e = tid; e < RL_PANEL; e += RIGHT_THREADS) {
+        const int row = e / RL_A_STRIDE, col = e - row * RL_A_STRIDE;
+        const bool in = col < 2 * CHI;
+        pn[e] = in ? A[row * AS + col] : 0.0;
+        if (pt != nullptr) pt[e] = in ? A[(col & 15) * AS + (col >> 4) * CHI + row] : 0.0;
+      }
+    }
     // T_i[c][b'] = sum_c' R[c][c'] A[b'][i][c']
     {
       const int c = tid >> 4, bp = tid & 15;

@@ -197,9 +197,10 @@ int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *theta_dev, 
  * [0] FP64 flops of the energy path as executed, [1] the survey count
  * 16 Dl Dr (Dl + Dr) per node-site of the prefix trie, [2] node-sites as
  * executed, [3] parent groups, [4] leaves, [5] largest environment slot count of
- * a level, [6] cut site of the split evaluation (-1: prefix trie only),
- * [7] / [8] flops / node-sites of the prefix trie alone, [9] prefix/suffix
- * pairs closed at the cut. */
+ * a level, [6] cut site of the single-cut split evaluation (-1: prefix trie
+ * only; the energy path then closes each word at its own cut when that needs
+ * fewer node-sites), [7] / [8] flops / node-sites of the prefix trie alone,
+ * [9] prefix/suffix pair closures. */
 int vqemps_plan_stats(const vqemps_ctx *ctx, int handle, double *stats);
 
 /* Split evaluation (no reference counterpart; the reference walks prefix tries

@@ -47,3 +47,31 @@ def test_captured_partition_energy_replays_bitwise(vq):
     g.replay()
     torch.cuda.synchronize()
     assert torch.equal(out, eng.partition_energy(ps, theta))
+
+
+@pytest.mark.parametrize("split", [True, False])
+def test_captured_split_real_levels_replay_bitwise(vq, split):
+    """40 qubits, real-arithmetic levels; with the split evaluation (per-term cuts,
+    environments kept in per-level regions) the suffix half runs on the engine's
+    second stream, forked from and joined into the captured stream: replays equal
+    direct calls bit for bit."""
+    from vqemps import workloads as VW
+    spec, words, coeffs, thetas = VW.batched_40q(seed=3, batch=8, terms=1500)
+    eng = vq.Engine(0, 16)
+    eng.set_split_mode(split)
+    eng.set_spec(spec)
+    eng.set_level_variant("real_pf")
+    ham = eng.set_hamiltonian(words, coeffs)
+    assert (eng.plan_stats(ham)["cut"] >= 0) == split
+    th = torch.tensor(thetas, device=eng.device)
+    out = torch.empty(8, dtype=torch.float64, device=eng.device)
+    g = eng.capture(lambda: eng.energy(ham, th, out=out, check_status=False))
+    rng = np.random.default_rng(5)
+    for _ in range(2):
+        new = thetas + rng.normal(scale=0.05, size=thetas.shape)
+        th.copy_(torch.from_numpy(new))
+        g.replay()
+        torch.cuda.synchronize()
+        direct = eng.energy(ham, torch.from_numpy(new).to(eng.device))
+        assert torch.equal(out, direct)
+    eng.close()

@@ -185,3 +185,4 @@ def test_real_routed_circuit_pair_equals_chain_and_dense(vq):
             psi = np.moveaxis(np.tensordot(m, psi, axes=([1], [op[1]])), 0, op[1])
     dense = O.dense_expectations(psi.reshape(-1), words).real
     np.testing.assert_allclose(out["pair"][1][0], dense, atol=1e-11)
+

@@ -67,6 +67,24 @@ def test_auto_split_at_40_qubits(vq, variant):
     assert abs(e1[3] - ref) <= 1e-9 * max(1.0, abs(ref))
 
 
+def test_per_term_cuts_at_40_qubits(vq):
+    """The benchmark's Hamiltonian: closing each word at its own cut needs fewer
+    node-sites than the single cut at site 20 (18,913); a batch of 32 states uses
+    it, and its energies and per-term values equal the prefix plan's for the real
+    and the complex level kernels."""
+    spec, words, coeffs, thetas = W.batched_40q(0, batch=32)
+    for variant in ("real_pf", "dmma3_pf"):
+        e1, pt1, st1 = _energies(vq, spec, words, coeffs, thetas, "auto", variant)
+        e0, pt0, st0 = _energies(vq, spec, words, coeffs, thetas, "off", variant)
+        assert st1["cut"] == 20 and st1["node_sites"] <= 16000 and st1["pairs"] > 3000
+        np.testing.assert_allclose(e1, e0, rtol=1e-12)
+        np.testing.assert_allclose(pt1, pt0, rtol=0, atol=1e-11)
+        # a small batch evaluates the same states with the single cut
+        e4, pt4, _ = _energies(vq, spec, words, coeffs, thetas[:4], "auto", variant)
+        np.testing.assert_allclose(e4, e1[:4], rtol=1e-12)
+        np.testing.assert_allclose(pt4, pt1[:4], rtol=0, atol=1e-11)
+
+
 def test_split_with_sampling_and_widths(vq):
     """Shot estimates use the split plan's analytic X/Y values; tiny widths and
     words ending on either side of the cut."""
