@@ -138,9 +138,11 @@ struct Hamiltonian {
   const int32_t *e_term_leaf() const { return mcut ? d_mc_term_leaf : cut >= 0 ? d_split_term_leaf : d_term_leaf; }
 };
 
-// As-soon-as-possible schedule of a circuit's two-site gates for the two-CTA gate
-// chain (evolve_pair_kernel), at most two gates per step on disjoint site pairs,
-// and the one-site gates each two-site gate folds in (see EvolveParams).
+// As-soon-as-possible schedule of a circuit's two-site gates for the K-CTA gate
+// chains (evolve_pair_kernel: K = 2, evolve_quad_real_kernel: K = 4), at most K
+// gates per step on disjoint site pairs (step t: sched[K t .. K t + K - 1]), and
+// the one-site gates each two-site gate folds in (see EvolveParams); the folding
+// does not depend on K.
 struct PairSched {
   std::vector<int32_t> sched, gate_q, qlist, tail_off;
   int nsteps = 0;
@@ -167,7 +169,7 @@ void mark_sigma_side(std::vector<DevGate> &gates) {
   }
 }
 
-PairSched build_pair_schedule(const std::vector<DevGate> &gates, int n) {
+PairSched build_pair_schedule(const std::vector<DevGate> &gates, int n, int K = 2) {
   PairSched ps;
   ps.gate_q.assign(4 * std::max<size_t>(gates.size(), 1), 0);
   std::vector<std::vector<int32_t>> pend(n);
@@ -186,13 +188,12 @@ PairSched build_pair_schedule(const std::vector<DevGate> &gates, int n) {
       pend[s + side].clear();
     }
     int t = std::max(last_step[s], last_step[s + 1]) + 1;
-    while (t < (int)count.size() && count[t] >= 2) ++t;
+    while (t < (int)count.size() && count[t] >= K) ++t;
     if (t == (int)count.size()) {
       count.push_back(0);
-      ps.sched.push_back(-1);
-      ps.sched.push_back(-1);
+      ps.sched.insert(ps.sched.end(), K, -1);
     }
-    ps.sched[2 * t + count[t]] = gi;
+    ps.sched[K * t + count[t]] = gi;
     ++count[t];
     last_step[s] = last_step[s + 1] = t;
   }
@@ -316,6 +317,8 @@ struct vqemps_ctx {
   bool panels_t_fresh = false;
   DevBuf<cplx> mflat_p, mflat_s;        // per-term-cut plan: level regions of the prefix / suffix half
   int level_launches = 0;               // kernels the last run_levels launched
+  int evolve_launches = 0;              // kernels the last launch_evolve launched
+  DevBuf<cplx> upend;                   // pending one-site products of the multi-CTA chains
   // The split evaluation's suffix half runs on a second stream, forked from and
   // joined back into the caller's stream (so graph capture sees both).
   cudaStream_t aux = nullptr;
@@ -337,14 +340,18 @@ struct vqemps_ctx {
   int grad_checkpoint = 8;              // gradient: keep every 8th level's environments
   int grad_mma = 2;                     // gradient levels: 0 SIMT, 1 FP64 DMMA, 2 DMMA with Gauss forward
   int split_mode = -1;                  // split evaluation: -1 when it saves work, 0 never, 1 always
-  int evolve_pair = -1;                 // gate chain: 1 two-CTA clusters, 0 one CTA, -1 by batch size
+  int evolve_pair = -1;                 // gate chain: 2 four-CTA clusters (real circuits), 1 two-CTA
+                                        // clusters, 0 one CTA, -1 by batch size
   int sm_count = 148;
   PairSched psched;
   int32_t *d_sched = nullptr, *d_gate_q = nullptr, *d_qlist = nullptr, *d_tail_off = nullptr;
+  int32_t *d_qsched = nullptr;          // four gates per step (evolve_quad_real_kernel)
+  int qsteps = 0;
+  int quad_clusters = -1;               // clusters of evolve_quad_real_kernel the GPU holds at once (-1: not queried)
   ~vqemps_ctx() {
     cudaFree(d_gates); cudaFree(d_mats); cudaFree(d_events); cudaFree(d_ev_off);
     cudaFree(d_ev_dims); cudaFree(d_slot_off); cudaFree(d_slot_list);
-    cudaFree(d_sched); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off);
+    cudaFree(d_sched); cudaFree(d_gate_q); cudaFree(d_qlist); cudaFree(d_tail_off); cudaFree(d_qsched);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (aux) cudaStreamDestroy(aux);
@@ -392,7 +399,8 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(evolve_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(evolve_pair_mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (const char *v = std::getenv("VQEMPS_EVOLVE"))
-    ctx->evolve_pair = std::strcmp(v, "chain") == 0 ? 0 : std::strcmp(v, "pair") == 0 ? 1 : -1;
+    ctx->evolve_pair = std::strcmp(v, "chain") == 0 ? 0 : std::strcmp(v, "pair") == 0 ? 1
+                       : std::strcmp(v, "quad") == 0 ? 2 : -1;
   cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
   cudaFuncSetAttribute(level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(LevelSmem));
@@ -632,12 +640,16 @@ extern "C" int vqemps_set_circuit(vqemps_ctx *ctx, int n, const vqemps_op *ops, 
     CUDA_TRY(ctx, upi(ctx->d_qlist, ps.qlist));
     CUDA_TRY(ctx, upi(ctx->d_tail_off, ps.tail_off));
     ctx->psched = std::move(ps);
+    const PairSched qs = build_pair_schedule(gates, n, 4);
+    CUDA_TRY(ctx, upi(ctx->d_qsched, qs.sched));
+    ctx->qsteps = qs.nsteps;
   }
   ctx->gates = std::move(gates);
   ctx->mats = std::move(mats);
   ctx->grad_ops = std::move(gops);
   ctx->bonds = bonds;
   ctx->n = n;
+  ctx->quad_clusters = -1;
   ctx->P = P;
   ctx->site_order = site_order;
   ctx->site_of_qubit = site_of;
@@ -1027,6 +1039,40 @@ static bool use_pair_chain(const vqemps_ctx *ctx, int B) {
   return ctx->evolve_pair > 0 || (ctx->evolve_pair < 0 && B <= 2 * ctx->sm_count);
 }
 
+// Four CTAs per state (circuits of real gates) when the four-gate schedule is
+// shorter than the two-gate one and all B clusters are resident at once (a second
+// wave would double the chain's time); forced by mode 2.
+static bool use_quad_chain(vqemps_ctx *ctx, int B) {
+  if (!ctx->real_circuit || ctx->evolve_pair == 0 || ctx->evolve_pair == 1) return false;
+  if (ctx->evolve_pair == 2) return true;
+  if (ctx->qsteps >= ctx->psched.nsteps) return false;
+  // measured on the 40-qubit benchmark circuit: four CTAs per state win while the
+  // GPU holds at most about four CTAs per SM (B <= 128: 1.09 against 1.29 ms); with
+  // more, the extra resident warps only wait at the CTA barriers (B = 256: 1.48
+  // against 1.44 ms with two CTAs per state)
+  if (B > ctx->sm_count) return false;
+  if (ctx->quad_clusters < 0) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(4 * 8 * ctx->sm_count);
+    cfg.blockDim = dim3(PAIR_THREADS);
+    cfg.dynamicSmemBytes = EvolveSmemReal::bytes(ctx->n);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 4;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, (void *)evolve_quad_real_kernel, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      nc = 0;
+    }
+    ctx->quad_clusters = nc;
+  }
+  return B <= ctx->quad_clusters;
+}
+
 static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaStream_t st) {
   EvolveParams ep{};
   ep.gates = ctx->d_gates;
@@ -1043,7 +1089,28 @@ static int launch_evolve(vqemps_ctx *ctx, const double *theta_dev, int B, cudaSt
   ep.max_bond = ctx->max_bond;
   ep.abs_cut = ctx->abs_cut;
   ep.rel_cut = ctx->rel_cut;
-  if (use_pair_chain(ctx, B)) {
+  ctx->evolve_launches = 1;
+  const bool quad = use_quad_chain(ctx, B);
+  if (quad || use_pair_chain(ctx, B)) {
+    // every two-site gate's pending one-site products, formed in parallel
+    CUDA_TRY(ctx, ctx->upend.ensure((size_t)B * std::max(ep.ngates, 1) * 8));
+    ep.gate_q = ctx->d_gate_q;
+    ep.qlist = ctx->d_qlist;
+    if (ep.ngates > 0) {
+      pending_kernel<<<dim3((ep.ngates + 127) / 128, B), 128, 0, st>>>(ep, ctx->upend.ptr);
+      CUDA_TRY(ctx, cudaGetLastError());
+      ctx->evolve_launches = 2;
+    }
+    ep.upend = ctx->upend.ptr;
+  }
+  if (quad) {
+    ep.sched = ctx->d_qsched;
+    ep.nsteps = ctx->qsteps;
+    ep.gate_q = ctx->d_gate_q;
+    ep.qlist = ctx->d_qlist;
+    ep.tail_off = ctx->d_tail_off;
+    evolve_quad_real_kernel<<<4 * B, PAIR_THREADS, EvolveSmemReal::bytes(ctx->n), st>>>(ep);
+  } else if (use_pair_chain(ctx, B)) {
     ep.sched = ctx->d_sched;
     ep.nsteps = ctx->psched.nsteps;
     ep.gate_q = ctx->d_gate_q;
@@ -1494,7 +1561,7 @@ static int launch_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st
 // in program order, -1 (default) two-CTA clusters while B <= the SM count.
 // Same states bit for bit.
 extern "C" int vqemps_set_evolve_mode(vqemps_ctx *ctx, int mode) {
-  if (!ctx || mode < -1 || mode > 1) return VQEMPS_INVALID;
+  if (!ctx || mode < -1 || mode > 2) return VQEMPS_INVALID;
   ctx->evolve_pair = mode;
   return VQEMPS_OK;
 }
@@ -1595,7 +1662,7 @@ extern "C" int vqemps_profile_energy(vqemps_ctx *ctx, int handle, const double *
   ms[1] = t[1];
   ms[3] = t[3];
   ms[2] = t[2] - t[3];   // launch_levels includes one reduction
-  *launches = 1 + 1 + ctx->level_launches + 1;   // gate chain, right environments, levels, reduction
+  *launches = ctx->evolve_launches + 1 + ctx->level_launches + 1;   // gate chain, right env, levels, reduction
   for (auto &e : ev) cudaEventDestroy(e);
   ctx->last_B = B;
   return VQEMPS_OK;

@@ -93,6 +93,10 @@ struct EvolveParams {
   // Mixed partition sets (the per-partition chain kernels): 1 where partition
   // k's circuit is of real gates (real-arithmetic Jacobi), 0 where complex.
   const int32_t *part_real;
+  // Multi-CTA chains of one circuit: the pending one-site products of every
+  // two-site gate, [B][ngates][8] (U_s then U_{s+1}), formed beforehand by
+  // pending_kernel (null: formed by one thread when the gate is applied).
+  const cplx *upend;
 };
 
 constexpr int EVOLVE_THREADS = 256;   // one-CTA gate chain
@@ -113,6 +117,25 @@ struct EvolveSmem {
   static constexpr int SCHED = MISC + 64;                  // 32 x 16 ints: Jacobi pairs of the gate
   static constexpr int PEND = SCHED + 32 * 16 * 4;         // n x 4 cplx pending 1q matrices
   static __host__ __device__ int bytes(int n) { return PEND + n * 4 * 16 + (n + 1) * 4 + 16; }
+};
+
+// The same tiles for real arithmetic in the multi-CTA chains (two_site_update_real
+// uses X, VT as 32 x 32 doubles, SA, SB as site tiles of doubles, G as 16
+// doubles) plus the 8 pending one-site entries U_s, U_{s+1}: 26.9 KiB, so eight
+// CTAs (64 registers each) fit an SM.
+struct EvolveSmemReal {
+  static constexpr int X = 0;                              // 32 x 32 doubles
+  static constexpr int VT = X + 32 * 32 * 8;
+  static constexpr int SA = VT + 32 * 32 * 8;              // site s tile, doubles
+  static constexpr int SB = SA + SITE_ELEMS * 8;
+  static constexpr int G = SB + SITE_ELEMS * 8;            // 4 x 4 doubles
+  static constexpr int NORM = G + 16 * 8;
+  static constexpr int SIG = NORM + 32 * 8;
+  static constexpr int PERM = SIG + 32 * 8;
+  static constexpr int MISC = PERM + 32 * 4;
+  static constexpr int SCHED = MISC + 64;
+  static constexpr int PEND = SCHED + 32 * 16 * 4;         // 8 cplx
+  static __host__ __device__ int bytes(int) { return PEND + 8 * 16; }
 };
 
 __device__ __forceinline__ void one_site_matrix(const DevGate &g, const cplx *mats,
@@ -829,6 +852,24 @@ __device__ __forceinline__ void pending_product(const EvolveParams &p, const dou
   }
 }
 
+// Pending one-site products of every two-site gate and state (grid: gate blocks x
+// states): one thread per gate, the same products in the same order as
+// pending_product inside the chain, so the states are unchanged bit for bit.
+__global__ void __launch_bounds__(128)
+pending_kernel(EvolveParams p, cplx *upend) {
+  const int b = blockIdx.y;
+  const int gi = blockIdx.x * 128 + threadIdx.x;
+  if (gi >= p.ngates) return;
+  const DevGate g = p.gates[gi];
+  if (g.kind != GATE_TWO) return;
+  const double *theta_b = p.theta + (size_t)b * p.P;
+  cplx u[8];
+  pending_product(p, theta_b, p.gate_q[4 * gi + 0], p.gate_q[4 * gi + 1], u);
+  pending_product(p, theta_b, p.gate_q[4 * gi + 2], p.gate_q[4 * gi + 3], u + 4);
+  cplx *dst = upend + ((size_t)b * p.ngates + gi) * 8;
+  for (int k = 0; k < 8; ++k) dst[k] = u[k];
+}
+
 // The gate chain of one state on a cluster of two CTAs. Two-site gates on
 // disjoint site pairs commute, so a precomputed as-soon-as-possible schedule of
 // at most two gates per step (one per CTA) replaces program order; each step
@@ -838,26 +879,26 @@ __device__ __forceinline__ void pending_product(const EvolveParams &p, const dou
 // in global memory (read past L1 with ld.global.cg, since the other CTA writes
 // them). Both CTAs take every step, whatever the status, so the barrier counts
 // always match; after a failure the remaining gates are skipped.
-template <int MODE>
+template <int MODE, int K, class SM>
 __device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char smem[];
-  cplx *X = reinterpret_cast<cplx *>(smem + EvolveSmem::X);
-  cplx *VT = reinterpret_cast<cplx *>(smem + EvolveSmem::VT);
-  cplx *SA = reinterpret_cast<cplx *>(smem + EvolveSmem::SA);
-  cplx *SB = reinterpret_cast<cplx *>(smem + EvolveSmem::SB);
-  cplx *G = reinterpret_cast<cplx *>(smem + EvolveSmem::G);
-  double *NORM = reinterpret_cast<double *>(smem + EvolveSmem::NORM);
-  double *SIG = reinterpret_cast<double *>(smem + EvolveSmem::SIG);
-  int *PERM = reinterpret_cast<int *>(smem + EvolveSmem::PERM);
-  int *MISC = reinterpret_cast<int *>(smem + EvolveSmem::MISC);
-  int *SCHED = reinterpret_cast<int *>(smem + EvolveSmem::SCHED);
-  cplx *U = reinterpret_cast<cplx *>(smem + EvolveSmem::PEND);     // 8 entries: U_s, U_{s+1}
+  cplx *X = reinterpret_cast<cplx *>(smem + SM::X);
+  cplx *VT = reinterpret_cast<cplx *>(smem + SM::VT);
+  cplx *SA = reinterpret_cast<cplx *>(smem + SM::SA);
+  cplx *SB = reinterpret_cast<cplx *>(smem + SM::SB);
+  cplx *G = reinterpret_cast<cplx *>(smem + SM::G);
+  double *NORM = reinterpret_cast<double *>(smem + SM::NORM);
+  double *SIG = reinterpret_cast<double *>(smem + SM::SIG);
+  int *PERM = reinterpret_cast<int *>(smem + SM::PERM);
+  int *MISC = reinterpret_cast<int *>(smem + SM::MISC);
+  int *SCHED = reinterpret_cast<int *>(smem + SM::SCHED);
+  cplx *U = reinterpret_cast<cplx *>(smem + SM::PEND);     // 8 entries: U_s, U_{s+1}
 
   const int tid = threadIdx.x;
   const int rank = (int)cluster.block_rank();
-  const int b = blockIdx.x >> 1;
+  const int b = blockIdx.x / K;
   const int part = p.st_part ? p.st_part[b] : 0;
   const bool part_real = MODE == CHAIN_PER_PARTITION && p.part_real[part] != 0;
   const int n = p.st_part ? p.part_n[part] : p.n;
@@ -866,15 +907,15 @@ __device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
   int32_t *bonds_b = p.bonds + (size_t)b * (p.n + 1);
   volatile int32_t *status_b = p.status + b;
 
-  // |init>^n product state and unit bonds, split between the two CTAs
-  for (int e = tid + rank * PAIR_THREADS; e < n * SITE_ELEMS; e += 2 * PAIR_THREADS) {
+  // |init>^n product state and unit bonds, split between the K CTAs
+  for (int e = tid + rank * PAIR_THREADS; e < n * SITE_ELEMS; e += K * PAIR_THREADS) {
     const int el = e % SITE_ELEMS;
     cplx v = cmake(0, 0);
     if (el == 0) v = p.init0;
     else if (el == CHI) v = p.init1;
     sites_b[e] = v;
   }
-  for (int x = tid + rank * PAIR_THREADS; x <= n; x += 2 * PAIR_THREADS) bonds_b[x] = 1;
+  for (int x = tid + rank * PAIR_THREADS; x <= n; x += K * PAIR_THREADS) bonds_b[x] = 1;
   if (rank == 0 && tid == 0) *status_b = ST_OK;
   __threadfence();
   cluster.sync();
@@ -882,13 +923,28 @@ __device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
   const int t0 = p.step_off ? p.step_off[part] : 0;
   const int t1 = p.step_off ? p.step_off[part + 1] : p.nsteps;
   const EvolveShared sh{X, VT, SA, SB, G, NORM, SIG, PERM, MISC, SCHED};
+  // precomputed pending products (p.upend): threads 0..7 hold the entries of this
+  // CTA's gate of the next step, loaded one step ahead
+  const cplx *upend_b = p.upend ? p.upend + (size_t)b * p.ngates * 8 : nullptr;
+  cplx unext = cmake(0, 0);
+  if (upend_b && tid < 8 && t0 < t1) {
+    const int g0 = p.sched[K * t0 + rank];
+    if (g0 >= 0) unext = upend_b[(size_t)g0 * 8 + tid];
+  }
   for (int t = t0; t < t1; ++t) {
-    const int gi = p.sched[2 * t + rank];
+    const int gi = p.sched[K * t + rank];
+    const cplx ucur = unext;
+    if (upend_b && tid < 8 && t + 1 < t1) {
+      const int gn = p.sched[K * (t + 1) + rank];
+      if (gn >= 0) unext = upend_b[(size_t)gn * 8 + tid];
+    }
     // the other CTA may be writing the status of this step: one vote per CTA
     const bool ok = __syncthreads_and(*status_b == ST_OK);
     if (gi >= 0 && ok) {
       const DevGate g = p.gates[gi];
-      if (tid == 0) {
+      if (upend_b) {
+        if (tid < 8) U[tid] = ucur;
+      } else if (tid == 0) {
         pending_product(p, theta_b, p.gate_q[4 * gi + 0], p.gate_q[4 * gi + 1], U);
         pending_product(p, theta_b, p.gate_q[4 * gi + 2], p.gate_q[4 * gi + 3], U + 4);
       }
@@ -902,10 +958,10 @@ __device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
     __threadfence();
     cluster.sync();
   }
-  // one-site gates after the last two-site gate on each site (sites split by parity)
+  // one-site gates after the last two-site gate on each site (site x on CTA x mod K)
   if (__syncthreads_and(*status_b == ST_OK)) {
     const int base = p.part_tail_off ? p.part_tail_off[part] : 0;
-    for (int x = rank; x < n; x += 2) {
+    for (int x = rank; x < n; x += K) {
       __syncthreads();
       if (tid == 0) pending_product(p, theta_b, p.tail_off[base + x], p.tail_off[base + x + 1], U);
       __syncthreads();
@@ -914,15 +970,23 @@ __device__ __forceinline__ void evolve_pair_body(const EvolveParams &p) {
   }
 }
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
-evolve_pair_kernel(EvolveParams p) { evolve_pair_body<CHAIN_COMPLEX>(p); }
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 4)
+evolve_pair_kernel(EvolveParams p) { evolve_pair_body<CHAIN_COMPLEX, 2, EvolveSmem>(p); }
 
 // The two-CTA chain for a circuit of real gates (real-arithmetic Jacobi SVD).
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
-evolve_pair_real_kernel(EvolveParams p) { evolve_pair_body<CHAIN_REAL>(p); }
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 4)
+evolve_pair_real_kernel(EvolveParams p) { evolve_pair_body<CHAIN_REAL, 2, EvolveSmem>(p); }
 
 // The two-CTA chain of a mixed partition set (arithmetic per partition).
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS)
-evolve_pair_mixed_kernel(EvolveParams p) { evolve_pair_body<CHAIN_PER_PARTITION>(p); }
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PAIR_THREADS, 4)
+evolve_pair_mixed_kernel(EvolveParams p) { evolve_pair_body<CHAIN_PER_PARTITION, 2, EvolveSmem>(p); }
+
+// A circuit of real gates on a cluster of four CTAs: up to four gates per step
+// (the layers of a nearest-neighbour ansatz overlap in a wavefront: the 40-qubit,
+// 4-layer benchmark circuit takes 45 steps instead of 80 with two CTAs), on the
+// compact real tiles so that eight CTAs fit an SM (all 4 x 256 CTAs of a
+// 256-state batch at once). Same gates, same code, same bits as the one-CTA chain.
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(PAIR_THREADS, 8)
+evolve_quad_real_kernel(EvolveParams p) { evolve_pair_body<CHAIN_REAL, 4, EvolveSmemReal>(p); }
 
 }  // namespace vqemps

@@ -3,6 +3,7 @@
   python -m vqemps.benchmarks partitions   # 64 uneven partitions + 1000/4096 Philox shots
   python -m vqemps.benchmarks gradient     # 64q, 20,000 terms, B = 32 energy + gradient
   python -m vqemps.benchmarks graphs       # CUDA-graph replay vs direct launches
+  python -m vqemps.benchmarks chain        # the gate chain per mode (one, two, four CTAs) and batch size
 
 Each prints one JSON line per measurement. Inputs are the seeded synthetic
 workloads of ``oracle.workloads`` (no public data set stands behind them).
@@ -160,13 +161,45 @@ def bench_graphs(reps: int = 50):
                               graph_ms=ms_g, speedup=ms / ms_g)), flush=True)
 
 
+def bench_chain(batches=(1, 16, 64, 128, 256), modes=("auto", "quad", "pair", "chain"), reps: int = 5,
+                sample_only: bool = False):
+    """The benchmark circuit's gate chain (40 qubits, 156 two-site gates) for each
+    evolve mode and batch size: the prepare phase of an energy call (CUDA events
+    inside the engine). ``sample_only`` runs one-shot sampling calls instead (gate
+    chain, right environments, sampler: no trie-level buffers), for profilers."""
+    from vqemps import profiling
+    spec, words, coeffs, thetas = W.batched_40q(seed=0, batch=max(batches))
+    for mode in modes:
+        for B in batches:
+            eng = vqemps.Engine(0, 16)
+            eng.set_evolve_mode(mode)
+            eng.set_spec(spec)
+            th = torch.tensor(thetas[:B], device=eng.device)
+            if sample_only:
+                for _ in range(reps):
+                    eng.sample(th, 1, 7)
+                torch.cuda.synchronize()
+            else:
+                ham = eng.set_hamiltonian(words, coeffs)
+                for _ in range(2):
+                    eng.energy(ham, th)
+                ph = profiling.phase_times(eng, ham, th, repeats=reps)
+                print(json.dumps(dict(workload="40q reverse_linear RY, 4 layers (156 two-site gates)", mode=mode,
+                                      batch=B, prepare_ms=ph["ms"]["prepare"],
+                                      states_per_s=B / ph["ms"]["prepare"] * 1e3)), flush=True)
+            eng.close()
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("which", choices=["partitions", "gradient", "graphs", "all"])
+    ap.add_argument("which", choices=["partitions", "gradient", "graphs", "chain", "all"])
     ap.add_argument("--reps", type=int, default=None, help="timed repetitions per measurement")
     ap.add_argument("--every", type=int, nargs="+", default=[8, 1], help="gradient checkpoint intervals")
     ap.add_argument("--plans", nargs="+", default=["auto", "off"], choices=["auto", "off", "on"],
                     help="gradient plans: split evaluation when it saves work (auto), prefix trie (off)")
+    ap.add_argument("--batches", type=int, nargs="+", default=[1, 16, 64, 128, 256], help="chain: batch sizes")
+    ap.add_argument("--modes", nargs="+", default=["auto", "quad", "pair", "chain"], help="chain: evolve modes")
+    ap.add_argument("--sample-only", action="store_true", help="chain: one-shot sampling calls, no output")
     args = ap.parse_args(argv)
     torch.cuda.set_device(0)
     if args.which in ("partitions", "all"):
@@ -175,6 +208,9 @@ def main(argv=None):
         bench_gradient(every=args.every, plans=args.plans, **({"reps": args.reps} if args.reps else {}))
     if args.which in ("graphs", "all"):
         bench_graphs(**({"reps": args.reps} if args.reps else {}))
+    if args.which in ("chain", "all"):
+        bench_chain(batches=args.batches, modes=args.modes, sample_only=args.sample_only,
+                    **({"reps": args.reps} if args.reps else {}))
 
 
 if __name__ == "__main__":

@@ -222,10 +222,13 @@ class Engine:
         return dict(zip(keys, list(out)))
 
     def set_evolve_mode(self, mode: str):
-        """Gate chain: 'pair' (two-CTA clusters on a schedule), 'chain' (one CTA, program
-        order) or 'auto' (pair while the batch has at most two states per SM; default)."""
-        check(self.ctx, self.lib.vqemps_set_evolve_mode(self.ctx, {"chain": 0, "pair": 1, "auto": -1}[mode]),
-              "set_evolve_mode")
+        """Gate chain: 'quad' (four-CTA clusters, circuits of real gates; others run
+        'pair'), 'pair' (two-CTA clusters on a schedule), 'chain' (one CTA, program
+        order) or 'auto' (default: quad for a circuit of real gates while all its
+        clusters fit the GPU at once, else pair while the batch has at most two
+        states per SM, else chain). All give the same states bit for bit."""
+        check(self.ctx, self.lib.vqemps_set_evolve_mode(
+            self.ctx, {"chain": 0, "pair": 1, "quad": 2, "auto": -1}[mode]), "set_evolve_mode")
 
     def set_split_mode(self, mode):
         """Split evaluation of Hamiltonians loaded afterwards: None/'auto' (when it

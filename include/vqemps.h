@@ -214,9 +214,12 @@ int vqemps_set_split_mode(vqemps_ctx *ctx, int mode);
 /* Gate chain (no reference counterpart; the reference applies gates one by one,
  * simulator_mps_dist.cu:1392-1406): 1 runs each state on a cluster of two CTAs
  * that apply two-site gates on disjoint site pairs concurrently, on an
- * as-soon-as-possible schedule built with the circuit; 0 runs one CTA per state
- * in program order; -1 (default) uses 1 while the batch has at most twice as
- * many states as the GPU has SMs, else 0. All give the same states bit for bit. */
+ * as-soon-as-possible schedule built with the circuit; 2 (circuits of real gates;
+ * others as 1) on a cluster of four CTAs, up to four gates per step; 0 runs one
+ * CTA per state in program order; -1 (default) uses 2 for a circuit of real gates
+ * while all clusters of four fit the GPU at once and the four-gate schedule is
+ * shorter, else 1 while the batch has at most twice as many states as the GPU has
+ * SMs, else 0. All give the same states bit for bit. */
 int vqemps_set_evolve_mode(vqemps_ctx *ctx, int mode);
 
 /* Copy the site tensors of state b of the last batched call to the host:

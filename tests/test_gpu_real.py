@@ -151,7 +151,7 @@ def test_real_routed_circuit_pair_equals_chain_and_dense(vq):
     words = ["".join(rng.choice(list("IXYZ"), 7)) for _ in range(50)]
     coeffs = rng.normal(size=50)
     out = {}
-    for mode in ("pair", "chain"):
+    for mode in ("pair", "chain", "quad"):
         eng = vq.Engine(0, 16)
         eng.set_evolve_mode(mode)
         eng.set_level_variant("real_pf")
@@ -160,8 +160,9 @@ def test_real_routed_circuit_pair_equals_chain_and_dense(vq):
         e, pt = eng.energy(ham, x, per_term=True)
         out[mode] = (e.cpu().numpy(), pt.cpu().numpy(), eng.sites(0), eng.bond_dims())
         eng.close()
-    assert np.array_equal(out["pair"][2], out["chain"][2]) and out["pair"][3] == out["chain"][3]
-    assert np.array_equal(out["pair"][0], out["chain"][0])
+    for mode in ("pair", "quad"):
+        assert np.array_equal(out[mode][2], out["chain"][2]) and out[mode][3] == out["chain"][3]
+        assert np.array_equal(out[mode][0], out["chain"][0])
     # the dense reference: U1 / U2 through their matrices
     psi = np.zeros(2 ** 7, dtype=complex)
     psi[0] = 1.0
@@ -186,3 +187,25 @@ def test_real_routed_circuit_pair_equals_chain_and_dense(vq):
     dense = O.dense_expectations(psi.reshape(-1), words).real
     np.testing.assert_allclose(out["pair"][1][0], dense, atol=1e-11)
 
+
+
+def test_quad_chain_equals_pair_and_chain_on_the_benchmark_circuit(vq):
+    """Four CTAs per state (up to four gates per step) on the 40-qubit benchmark
+    circuit: the states of 16 parameter sets equal the two-CTA and one-CTA chains'
+    bit for bit, and so do the energies."""
+    from vqemps import workloads as VW
+    spec, words, coeffs, thetas = VW.batched_40q(seed=0, batch=16)
+    out = {}
+    for mode in ("quad", "pair", "chain"):
+        eng = vq.Engine(0, 16)
+        eng.set_evolve_mode(mode)
+        eng.set_spec(spec)
+        eng.set_level_variant("real_pf")
+        ham = eng.set_hamiltonian(words, coeffs)
+        e = eng.energy(ham, torch.tensor(thetas, device=eng.device)).cpu().numpy()
+        out[mode] = (e, [eng.sites(b) for b in (0, 7, 15)], eng.bond_dims())
+        eng.close()
+    for mode in ("pair", "chain"):
+        assert np.array_equal(out["quad"][0], out[mode][0])
+        assert all(np.array_equal(a, c) for a, c in zip(out["quad"][1], out[mode][1]))
+        assert out["quad"][2] == out[mode][2]
