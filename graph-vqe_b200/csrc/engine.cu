@@ -121,7 +121,6 @@ struct Hamiltonian {
   long long mp_slots = 0, ms_slots = 0, mc_node_sites = 0, mc_groups_total = 0;
   int mc_max_slot = 1;
   double mc_flops = 0.0;
-  std::vector<int32_t> term_node;        // n x T: term t's prefix-trie node at level s (kept for the deferred build)
   DevGroup *d_mp_groups = nullptr, *d_ms_groups = nullptr;
   DevNode *d_mp_nodes = nullptr, *d_ms_nodes = nullptr;
   DevPair *d_mc_pairs = nullptr;
@@ -768,7 +767,6 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   h->node_off.assign(n + 1, 0);
   h->nslot.assign(n, 0);
   h->term_slot.assign((size_t)n * T, -1);   // level-major: one level's writes stay in one row
-  h->term_node.assign((size_t)n * T, -1);
   h->level_flops.assign(n, 0.0);
   const std::vector<int> &bd = ctx->bonds;
   for (int s = 0; s < n; ++s) {
@@ -818,10 +816,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         h->nodes[h->node_off[s] + k].env_slot = slot_of[k];
       }
     h->nslot[s] = slots;
-    for (size_t j = 0; j < active.size(); ++j) {
-      h->term_slot[(size_t)s * T + active[j]] = slot_of[node_of[j]];
-      h->term_node[(size_t)s * T + active[j]] = node_of[j];
-    }
+    for (size_t j = 0; j < active.size(); ++j) h->term_slot[(size_t)s * T + active[j]] = slot_of[node_of[j]];
     h->max_slot = std::max(h->max_slot, slots);
     // groups: consecutive nodes with the same parent
     {
@@ -865,7 +860,6 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   h->node_off[n] = (int)h->nodes.size();
   build_split_plan(*h, code, last, ctx->bonds, ctx->split_mode);
   std::vector<int32_t>().swap(h->term_slot);
-  if (!h->mc_pending) std::vector<int32_t>().swap(h->term_node);
   // upload: every plan array is a 256-byte aligned slice of ONE device
   // allocation, filled by one copy of a packed host image (tens of separate
   // allocations and copies cost more than the plan build itself at 40,000 terms)
@@ -933,7 +927,6 @@ static int ensure_multicut(vqemps_ctx *ctx, Hamiltonian *h) {
   h->mc_pending = false;
   CUDA_TRY(ctx, cudaSetDevice(ctx->device));
   build_multicut_plan(*h);
-  std::vector<int32_t>().swap(h->term_node);
   std::vector<int32_t>().swap(h->mc_rslot);
   std::vector<int32_t>().swap(h->mc_sid_count);
   if (!h->mc_built) return VQEMPS_OK;

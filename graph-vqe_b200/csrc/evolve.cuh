@@ -121,8 +121,7 @@ struct EvolveSmem {
 
 // The same tiles for real arithmetic in the multi-CTA chains (two_site_update_real
 // uses X, VT as 32 x 32 doubles, SA, SB as site tiles of doubles, G as 16
-// doubles) plus the 8 pending one-site entries U_s, U_{s+1}: 26.9 KiB, so eight
-// CTAs (64 registers each) fit an SM.
+// doubles) plus the 8 pending one-site entries U_s, U_{s+1}: 26.9 KiB.
 struct EvolveSmemReal {
   static constexpr int X = 0;                              // 32 x 32 doubles
   static constexpr int VT = X + 32 * 32 * 8;
@@ -984,9 +983,10 @@ evolve_pair_mixed_kernel(EvolveParams p) { evolve_pair_body<CHAIN_PER_PARTITION,
 // A circuit of real gates on a cluster of four CTAs: up to four gates per step
 // (the layers of a nearest-neighbour ansatz overlap in a wavefront: the 40-qubit,
 // 4-layer benchmark circuit takes 45 steps instead of 80 with two CTAs), on the
-// compact real tiles so that eight CTAs fit an SM (all 4 x 256 CTAs of a
-// 256-state batch at once). Same gates, same code, same bits as the one-CTA chain.
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(PAIR_THREADS, 8)
+// compact real tiles. The engine takes it while the batch needs at most about
+// four CTAs per SM (beyond that the extra resident warps only wait at the CTA
+// barriers). Same gates, same code, same bits as the one-CTA chain.
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(PAIR_THREADS, 4)
 evolve_quad_real_kernel(EvolveParams p) { evolve_pair_body<CHAIN_REAL, 4, EvolveSmemReal>(p); }
 
 }  // namespace vqemps

@@ -133,7 +133,7 @@ def bench_gradient(reps: int = 3, every=(8, 1), plans=("auto", "off")):
             ms_e = _events_ms(lambda: eng.energy(ham, th, check_status=False), reps, stream)
             print(json.dumps(dict(workload="64q linear RY, 320 angles, 20000 terms (wmax 6), energy + gradient",
                                   batch=B, plan="split" if stats["cut"] >= 0 else "prefix", cut=stats["cut"],
-                                  node_sites=stats["node_sites"], checkpoint_every=k, ms_per_call=ms,
+                                  energy_plan_node_sites=stats["node_sites"], checkpoint_every=k, ms_per_call=ms,
                                   grads_per_s=B / (ms * 1e-3), energy_only_ms=ms_e, grad_over_energy=ms / ms_e,
                                   workspace_growth_bytes=int(used))), flush=True)
         eng.close()

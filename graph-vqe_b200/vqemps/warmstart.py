@@ -287,7 +287,20 @@ def main(argv=None):
     else:
         rows, summary = evaluate(args.params, args.count, n=args.n, terms=args.terms)
         if args.out:
-            Path(args.out).write_text(json.dumps(dict(rows=rows, summary=summary)))
+            ratios = [r["ratio"] for r in rows if r["ratio"] is not None]
+            med = lambda key: float(np.median([r[key] for r in rows if r.get(key) is not None]))
+            Path(args.out).write_text(json.dumps(dict(
+                command=f"cd graph-vqe_b200 && python -m vqemps.warmstart evaluate --params {args.params} "
+                        f"--count {args.count} --n {args.n} --terms {args.terms}",
+                instances=f"{args.count} unseen Hamiltonians: vqemps.workloads.warm_start_test_problem(seed, "
+                          f"n={args.n}, terms={args.terms}), seeds 900000..{900000 + args.count - 1}",
+                weights=Path(args.params).name,
+                summary=summary,
+                ratio_percentiles={str(q): float(np.percentile(ratios, q)) for q in (10, 25, 50, 75, 90)}
+                if ratios else None,
+                plain_s_median=med("plain_s"), learned_reached_s_median=med("learned_reached_s"),
+                learned_setup_s_median=med("learned_setup_s"),
+                ratios=[round(x, 4) for x in ratios]), indent=1))
 
 
 if __name__ == "__main__":
