@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <future>
 #include <array>
 #include <map>
 #include <memory>
@@ -756,6 +757,13 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
       h->term_leaf[t] = h->identity_leaf;
       h->leaf_coef[h->identity_leaf] += coeffs[t];
     }
+  // the split plan's suffix trie needs only the words: build it on a second host
+  // thread while this one builds the prefix trie
+  const bool want_split = ctx->split_mode != 0 && n >= 3 && T > 0;
+  std::future<SuffixTrie> suffix;
+  if (want_split)
+    suffix = std::async(std::launch::async, build_suffix_trie, n, T, std::cref(code), std::cref(last),
+                        std::cref(ctx->bonds));
   // level-by-level construction over the sorted order
   std::vector<int> active;  // words (sorted order) still on a path at this level
   for (int t : order)
@@ -858,7 +866,7 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
   }
   h->group_off[n] = (int)h->groups.size();
   h->node_off[n] = (int)h->nodes.size();
-  build_split_plan(*h, code, last, ctx->bonds, ctx->split_mode);
+  build_split_plan(*h, want_split ? suffix.get() : SuffixTrie{}, code, last, ctx->bonds, ctx->split_mode);
   std::vector<int32_t>().swap(h->term_slot);
   // upload: every plan array is a 256-byte aligned slice of ONE device
   // allocation, filled by one copy of a packed host image (tens of separate
