@@ -353,7 +353,7 @@ def main():
                     ms_per_step=ms_per_step, higher_is_better=True, scaling="weak", vs_baseline=None,
                     dtype="f64", data="synthetic",
                     config=dict(WORKLOAD, global_batch=args.batch * world, parallelism=f"replicas x{world}",
-                                l2="working set per step > L2 (env buffers ~4 GB): no flush needed",
+                                l2="working set per step > L2 (level environments ~6 GB): no flush needed",
                                 plain_evals_per_s=plain_rate, batched_over_plain=value / world / plain_rate,
                                 flops_per_eval=flops_eval, survey_flops_per_eval=stats["flops_survey"],
                                 trie_node_sites=stats["node_sites"],
