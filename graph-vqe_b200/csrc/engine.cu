@@ -421,6 +421,10 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
                        (int)sizeof(GradBwdMmaSmem));
   cudaFuncSetAttribute(grad_fwd_level_mma3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradFwdMmaSmem));
+  cudaFuncSetAttribute(grad_fwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(GradFwdMmaSmem));
+  cudaFuncSetAttribute(grad_bwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(GradBwdMmaSmem));
   if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT"))
     ctx->grad_mma = std::strcmp(v, "simt") == 0 ? 0 : std::strcmp(v, "dmma") == 0 ? 1 : 2;
   // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the

@@ -38,10 +38,13 @@ __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int 
 }
 
 // S panel [S_0 | S_1] = E [A_0 | A_1] (16 x 32, K = 16) into padded S[i][row][col];
-// GAUSS: three real products per complex product (k1 = Yr (Xr + Xi),
-// k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2).
-template <bool GAUSS = false>
+// KIND 1 (Gauss): three real products per complex product (k1 = Yr (Xr + Xi),
+// k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2); KIND 0:
+// four; KIND 2: A real (a circuit of real gates), two -- the four-product sums
+// without their exact-zero terms, so the same bits.
+template <int KIND = 0>
 __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
+  constexpr bool GAUSS = KIND == 1;
   double sr[2][4][2], si[2][4][2], s3[GAUSS ? 2 : 1][4][2];
 #pragma unroll
   for (int rt = 0; rt < 2; ++rt)
@@ -69,6 +72,9 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
           dmma(sr[rt][ct][0], sr[rt][ct][1], er + ei, pf[ct].x);                 // k1
           dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y - pf[ct].x);           // k2
           dmma(s3[rt][ct][0], s3[rt][ct][1], ei, pf[ct].x + pf[ct].y);           // k3
+        } else if constexpr (KIND == 2) {
+          dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
+          dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
         } else {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
@@ -92,7 +98,7 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
       }
 }
 
-template <bool GAUSS>
+template <int KIND>
 __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradFwdMmaSmem &sm = *reinterpret_cast<GradFwdMmaSmem *>(smem_raw);
   const int b = blockIdx.y;
@@ -123,7 +129,7 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    mma_panel_EA<GAUSS>(E, A, S, g, t);
+    mma_panel_EA<KIND>(E, A, S, g, t);
     __syncwarp();   // E is dead and S complete: prefetch the next parent
     if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
     cp_async_commit();
@@ -133,10 +139,10 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
       // X/Y: t1 = A_1^H S_0 = t0^H through the S panel (as level_mma_pf_body).
       double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
       if (cls == 0) {
-        class_tiles<GAUSS, true>(A, 0, S, 0, ar, ai, g, t);
-        class_tiles<GAUSS, true>(A, CHI, S, 1, br, bi, g, t);
+        class_tiles<KIND, true>(A, 0, S, 0, ar, ai, g, t);
+        class_tiles<KIND, true>(A, CHI, S, 1, br, bi, g, t);
       } else {
-        class_tiles<GAUSS, false>(A, 0, S, 1, ar, ai, g, t);
+        class_tiles<KIND, false>(A, 0, S, 1, ar, ai, g, t);
         __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
@@ -230,14 +236,22 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
 __global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
 grad_fwd_level_mma_kernel(GradLevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_fwd_level_mma_body<false>(p, smem_raw);
+  grad_fwd_level_mma_body<0>(p, smem_raw);
 }
 
 // Forward gradient level with Gauss's three-product complex multiply.
 __global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
 grad_fwd_level_mma3_kernel(GradLevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_fwd_level_mma_body<true>(p, smem_raw);
+  grad_fwd_level_mma_body<1>(p, smem_raw);
+}
+
+// Forward gradient level for a circuit of real gates: real site tiles, two real
+// products per complex one (the four-product kernel's bits).
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_fwd_level_real_a_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_fwd_level_mma_body<2>(p, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,9 +272,10 @@ struct GradBwdMmaSmem {
   cplx D[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];   // the class's D pair [d][k][c]
 };
 
-__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
-grad_bwd_level_mma_kernel(GradLevelParams p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+// REAL_A: a circuit of real gates -- the products with the site tile (Y = A D and
+// Ebar = Y A^H) skip the terms of its zero imaginary parts (same bits).
+template <bool REAL_A>
+__device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradBwdMmaSmem &sm = *reinterpret_cast<GradBwdMmaSmem *>(smem_raw);
   const int b = blockIdx.y;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -355,9 +370,9 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
           for (int ct = 0; ct < 4; ++ct) {
             const cplx a = af[ct >> 1][rt], d = df[ct];
             dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
-            dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
+            if (!REAL_A) dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
             dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
-            dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
+            if (!REAL_A) dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
           }
       }
     }
@@ -420,9 +435,9 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
             if (rt == 1 && ct == 0) continue;
             // Y conj(A): re = Yr Ar + Yi Ai, im = Yi Ar - Yr Ai
             dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
-            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
+            if (!REAL_A) dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
             dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
-            dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
+            if (!REAL_A) dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
           }
       }
       cplx *dst = grp.parent_slot >= 0 ? p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS
@@ -461,5 +476,17 @@ grad_bwd_level_mma_kernel(GradLevelParams p) {
   }
 }
 
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_bwd_level_mma_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_bwd_level_mma_body<false>(p, smem_raw);
+}
+
+// Backward gradient level for a circuit of real gates (real site tiles).
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+grad_bwd_level_real_a_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_bwd_level_mma_body<true>(p, smem_raw);
+}
 
 }  // namespace vqemps
