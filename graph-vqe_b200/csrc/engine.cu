@@ -329,8 +329,10 @@ struct vqemps_ctx {
   DevBuf<double> analytic_stage;
   DevBuf<cplx> grad_sites, grad_envs, grad_seg, grad_bar0, grad_bar1, grad_sitebar, grad_partial, grad_leafsum;
   // split gradient: transposed sites, suffix environments (all levels), suffix
-  // cotangents (ping-pong), cotangents of R_{s+1} from the suffix roots
-  DevBuf<cplx> grad_sites_t, grad_senv, grad_sbar0, grad_sbar1, grad_rootbar;
+  // cotangents (ping-pong), cotangents of R_{s+1} from the suffix roots, the
+  // suffix backward's site partials (it runs beside the prefix half on the
+  // second stream) and the left sweep's F at the cut
+  DevBuf<cplx> grad_sites_t, grad_senv, grad_sbar0, grad_sbar1, grad_rootbar, grad_partial_s, grad_fstate;
   DevBuf<double> grad_stage;
   int last_B = 0;
   int forced_variant = -1;              // level kernel variant, -1: autotune
@@ -453,7 +455,8 @@ extern "C" int vqemps_destroy(vqemps_ctx *ctx) {
   ctx->grad_bar1.release(); ctx->grad_sitebar.release(); ctx->grad_stage.release();
   ctx->grad_partial.release(); ctx->grad_leafsum.release(); ctx->grad_seg.release();
   ctx->grad_sites_t.release(); ctx->grad_senv.release(); ctx->grad_sbar0.release();
-  ctx->grad_sbar1.release(); ctx->grad_rootbar.release();
+  ctx->grad_sbar1.release(); ctx->grad_rootbar.release(); ctx->grad_partial_s.release();
+  ctx->grad_fstate.release();
   delete ctx;
   return VQEMPS_OK;
 }

@@ -381,18 +381,21 @@ split_pair_bwd_kernel(const cplx *__restrict__ left, size_t left_stride, const c
 // ---------------------------------------------------------------------------
 // rootbar (may be null): cotangents of R_{q+1} from the split evaluation's
 // suffix roots (bar convention, conjugated into F); accumulate adds the site
-// cotangents to sitebar instead of writing them.
+// cotangents to sitebar instead of writing them.  The sweep covers sites
+// q0 .. q1-1: it starts from fstate[b] when q0 > 0 and stores F_{q1} there when
+// q1 < n, so a sweep split at the cut gives the same bits as one sweep.
 __global__ void __launch_bounds__(256)
 grad_suffix_kernel(const cplx *__restrict__ sites, const cplx *__restrict__ right,
                    const cplx *__restrict__ leafsum, const cplx *__restrict__ rootbar,
-                   double identity_coef, int n, int accumulate, cplx *__restrict__ sitebar) {
+                   double identity_coef, int n, int accumulate, cplx *__restrict__ sitebar, int q0, int q1,
+                   cplx *__restrict__ fstate) {
   __shared__ cplx A[SITE_ELEMS];
   __shared__ cplx F[ENV_ELEMS];
   __shared__ cplx Rc[ENV_ELEMS];
   __shared__ cplx Tm[SITE_ELEMS];
   const int b = blockIdx.x, tid = threadIdx.x;
-  F[tid] = cmake(tid == 0 ? identity_coef : 0.0, 0.0);
-  for (int q = 0; q < n; ++q) {
+  F[tid] = q0 > 0 ? fstate[(size_t)b * ENV_ELEMS + tid] : cmake(tid == 0 ? identity_coef : 0.0, 0.0);
+  for (int q = q0; q < q1; ++q) {
     const cplx *ag = sites + ((size_t)b * n + q) * SITE_ELEMS;
     A[tid] = ag[tid];
     A[tid + 256] = ag[tid + 256];
@@ -428,6 +431,7 @@ grad_suffix_kernel(const cplx *__restrict__ sites, const cplx *__restrict__ righ
     }
     __syncthreads();
   }
+  if (q1 < n) fstate[(size_t)b * ENV_ELEMS + tid] = F[tid];
 }
 
 // ---------------------------------------------------------------------------
