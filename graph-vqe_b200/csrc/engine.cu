@@ -1312,6 +1312,7 @@ static int run_levels_mcut(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t 
     lp.n = n;
     lp.s = s;
     lp.suffix = 1;
+    lp.flip = s & 1;
     lp.panels = ctx->panels_t.ptr;
     lp.right_real = ctx->right_real.ptr;
     lp.status = ctx->status.ptr;
@@ -1337,6 +1338,7 @@ static int run_levels_mcut(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t 
     lp.nleaf_total = nleaf;
     lp.n = n;
     lp.s = s;
+    lp.flip = s & 1;
     lp.panels = ctx->panels.ptr;
     lp.right_real = ctx->right_real.ptr;
     lp.status = ctx->status.ptr;
@@ -1412,6 +1414,7 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
       lp.n = n;
       lp.s = s;
       lp.suffix = 1;
+      lp.flip = s & 1;
       lp.panels = ctx->panels_t.ptr;
       lp.right_real = ctx->right_real.ptr;
       lp.status = ctx->status.ptr;
@@ -1439,6 +1442,7 @@ static int run_levels(vqemps_ctx *ctx, Hamiltonian &h, int B, cudaStream_t st, i
     lp.nleaf_total = nleaf;
     lp.n = n;
     lp.s = s;
+    lp.flip = s & 1;
     lp.panels = ctx->panels.ptr;
     lp.right_real = ctx->right_real.ptr;
     lp.status = ctx->status.ptr;

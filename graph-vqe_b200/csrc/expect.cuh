@@ -151,6 +151,10 @@ struct LevelParams {
   const double *panels;
   const double *right_real;
   int32_t *status;
+  // Nonzero: CTA row blockIdx.y works on state gridDim.y - 1 - blockIdx.y
+  // (real-arithmetic levels). Consecutive levels alternate, so a level first
+  // reads the parents its predecessor wrote last, while they are still in L2.
+  int flip;
 };
 
 struct LevelSmem {

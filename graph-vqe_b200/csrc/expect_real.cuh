@@ -188,7 +188,7 @@ level_real_pf_kernel(LevelParams p, int groups_per_warp) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   LevelRealSmem &sm = *reinterpret_cast<LevelRealSmem *>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int b = blockIdx.y;
+  const int b = p.flip ? (int)(gridDim.y - 1 - blockIdx.y) : (int)blockIdx.y;
   const int stride = gridDim.x * RL_WARPS;
   const int first = blockIdx.x * RL_WARPS + warp;
   int count = 0;
