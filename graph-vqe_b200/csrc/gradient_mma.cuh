@@ -41,9 +41,11 @@ __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int 
 // KIND 1 (Gauss): three real products per complex product (k1 = Yr (Xr + Xi),
 // k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2); KIND 0:
 // four; KIND 2: A real (a circuit of real gates), two -- the four-product sums
-// without their exact-zero terms, so the same bits.
+// without their exact-zero terms, so the same bits; KIND 3: A real and E of one
+// kind, i^k Er (real for even k, imaginary for odd: odd = k & 1), one -- KIND 2
+// without the products of E's zero part (same bits again).
 template <int KIND = 0>
-__device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
+__device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t, bool odd = false) {
   constexpr bool GAUSS = KIND == 1;
   double sr[2][4][2], si[2][4][2], s3[GAUSS ? 2 : 1][4][2];
 #pragma unroll
@@ -75,6 +77,8 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
         } else if constexpr (KIND == 2) {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
+        } else if constexpr (KIND == 3) {
+          dmma(sr[rt][ct][0], sr[rt][ct][1], odd ? ei : er, pf[ct].x);
         } else {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
@@ -93,6 +97,7 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
         const int col = ct * 8 + 2 * t + j;
         cplx v;
         if constexpr (GAUSS) v = cmake(sr[rt][ct][j] - s3[rt][ct][j], sr[rt][ct][j] + si[rt][ct][j]);
+        else if constexpr (KIND == 3) v = odd ? cmake(0.0, sr[rt][ct][j]) : cmake(sr[rt][ct][j], 0.0);
         else v = cmake(sr[rt][ct][j], si[rt][ct][j]);
         S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = v;
       }
@@ -129,7 +134,13 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    mma_panel_EA<KIND>(E, A, S, g, t);
+    // KIND 3: the parent's phase k (from its first child) says whether E is real or imaginary
+    bool odd = false;
+    if constexpr (KIND == 3) {
+      const DevNode n0 = p.nodes[grp.child_begin];
+      odd = ((n0.phase - (n0.code == 2 ? 1 : 0)) & 1) != 0;
+    }
+    mma_panel_EA<KIND>(E, A, S, g, t, odd);
     __syncwarp();   // E is dead and S complete: prefetch the next parent
     if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
     cp_async_commit();
@@ -139,10 +150,16 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
       // X/Y: t1 = A_1^H S_0 = t0^H through the S panel (as level_mma_pf_body).
       double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
       if (cls == 0) {
-        class_tiles<KIND, true>(A, 0, S, 0, ar, ai, g, t);
-        class_tiles<KIND, true>(A, CHI, S, 1, br, bi, g, t);
+        if constexpr (KIND == 3) {
+          class_tiles_pure<true>(A, 0, S, 0, ar, ai, g, t, odd);
+          class_tiles_pure<true>(A, CHI, S, 1, br, bi, g, t, odd);
+        } else {
+          class_tiles<KIND, true>(A, 0, S, 0, ar, ai, g, t);
+          class_tiles<KIND, true>(A, CHI, S, 1, br, bi, g, t);
+        }
       } else {
-        class_tiles<KIND, false>(A, 0, S, 1, ar, ai, g, t);
+        if constexpr (KIND == 3) class_tiles_pure<false>(A, 0, S, 1, ar, ai, g, t, odd);
+        else class_tiles<KIND, false>(A, 0, S, 1, ar, ai, g, t);
         __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
@@ -246,12 +263,13 @@ grad_fwd_level_mma3_kernel(GradLevelParams p) {
   grad_fwd_level_mma_body<1>(p, smem_raw);
 }
 
-// Forward gradient level for a circuit of real gates: real site tiles, two real
-// products per complex one (the four-product kernel's bits).
+// Forward gradient level for a circuit of real gates: real site tiles and
+// environments i^k Er, one real product per complex one where the four-product
+// kernel issues four (its bits).
 __global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
 grad_fwd_level_real_a_kernel(GradLevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_fwd_level_mma_body<2>(p, smem_raw);
+  grad_fwd_level_mma_body<3>(p, smem_raw);
 }
 
 // ---------------------------------------------------------------------------
@@ -273,7 +291,9 @@ struct GradBwdMmaSmem {
 };
 
 // REAL_A: a circuit of real gates -- the products with the site tile (Y = A D and
-// Ebar = Y A^H) skip the terms of its zero imaginary parts (same bits).
+// Ebar = Y A^H) skip the terms of its zero imaginary parts, and the site
+// cotangent E Y those of E's zero part (E = i^k Er is real or imaginary; the
+// cotangents mix both kinds): the same bits.
 template <bool REAL_A>
 __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradBwdMmaSmem &sm = *reinterpret_cast<GradBwdMmaSmem *>(smem_raw);
@@ -312,6 +332,11 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
     const DevGroup grp = p.groups[gidx];
     int idx_child[4] = {-1, -1, -1, -1};
     for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
+    bool odd = false;   // REAL_A: E imaginary (the parent's phase, from its first child)
+    if (REAL_A) {
+      const DevNode n0 = p.nodes[grp.child_begin];
+      odd = ((n0.phase - (n0.code == 2 ? 1 : 0)) & 1) != 0;
+    }
     // Y_o = sum over classes of A_src(o) D_src(o)
     double yr[2][4][2], yi[2][4][2];
 #pragma unroll
@@ -400,10 +425,17 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
         for (int ct = 0; ct < 4; ++ct) {
           const cplx x = ef[rt], d = yf[ct];
-          dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
-          dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
-          dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
-          dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
+          if (REAL_A) {
+            // even: re += Er Yr, im += Er Yi; odd: re += -Ei Yi, im += Ei Yr
+            const double xs = odd ? x.y : x.x;
+            dmma(abr[rt][ct][0], abr[rt][ct][1], odd ? -xs : xs, odd ? d.y : d.x);
+            dmma(abi[rt][ct][0], abi[rt][ct][1], xs, odd ? d.x : d.y);
+          } else {
+            dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
+            dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
+            dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
+            dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
+          }
         }
     }
     __syncwarp();   // E is consumed: prefetch the next parent
