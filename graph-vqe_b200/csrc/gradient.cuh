@@ -349,17 +349,21 @@ __global__ void partial_sum_t_kernel(const cplx *__restrict__ partial, int parts
 // weight c (the pair's leaf coefficient): Lbar[j] = sum_p c_p conj(R[rs_p]) over
 // the pairs of prefix slot j, Rbar[r] = sum_p c_p conj(L[ls_p]) over those of
 // suffix slot r, each in pair order. Block (slot, state), thread per element.
+// sign (may be null): Re(i^(kL + kR)) per pair; pairs where it is zero are left
+// out -- for real states their value is zero at every angle (the cotangents of
+// the real-gate gradient, whose imaginary-part bits they would only touch).
 __global__ void __launch_bounds__(ENV_ELEMS)
 split_pair_bwd_kernel(const cplx *__restrict__ left, size_t left_stride, const cplx *__restrict__ right,
                       size_t right_stride, const int32_t *__restrict__ pairs, const double *__restrict__ coef,
                       const int32_t *__restrict__ pl_off, int nls, const int32_t *__restrict__ pr_off,
                       const int32_t *__restrict__ pr_idx, cplx *__restrict__ lbar, size_t lbar_stride,
-                      cplx *__restrict__ rbar, size_t rbar_stride) {
+                      cplx *__restrict__ rbar, size_t rbar_stride, const double *__restrict__ sign) {
   const int b = blockIdx.y, e = threadIdx.x;
   const int j = blockIdx.x;
   cplx acc = cmake(0, 0);
   if (j < nls) {
     for (int k = pl_off[j]; k < pl_off[j + 1]; ++k) {
+      if (sign && sign[k] == 0.0) continue;
       const cplx r = right[(size_t)b * right_stride + (size_t)pairs[3 * k + 1] * ENV_ELEMS + e];
       acc = cadd(acc, cscale(cconj(r), coef[pairs[3 * k + 2]]));
     }
@@ -368,6 +372,7 @@ split_pair_bwd_kernel(const cplx *__restrict__ left, size_t left_stride, const c
     const int r = j - nls;
     for (int q = pr_off[r]; q < pr_off[r + 1]; ++q) {
       const int k = pr_idx[q];
+      if (sign && sign[k] == 0.0) continue;
       const cplx l = left[(size_t)b * left_stride + (size_t)pairs[3 * k] * ENV_ELEMS + e];
       acc = cadd(acc, cscale(cconj(l), coef[pairs[3 * k + 2]]));
     }

@@ -290,10 +290,17 @@ struct GradBwdMmaSmem {
   cplx D[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];   // the class's D pair [d][k][c]
 };
 
-// REAL_A: a circuit of real gates -- the products with the site tile (Y = A D and
-// Ebar = Y A^H) skip the terms of its zero imaginary parts, and the site
-// cotangent E Y those of E's zero part (E = i^k Er is real or imaginary; the
-// cotangents mix both kinds): the same bits.
+// REAL_A: a circuit of real gates. Its environments are i^k Er: real for even
+// phase k, imaginary for odd. A word with an odd number of Y's has the value
+// zero at every angle, and so has a pair closure of odd phase sum; their
+// cotangents reach only the imaginary parts of the site cotangents, which a
+// gradient with respect to real gate angles never reads. Left out (their leaf
+// weights taken as zero here, odd pairs masked by split_pair_bwd_kernel), every
+// cotangent is of its node's kind, like the environment, so each complex product
+// with the site tile, E or Y is one real product: D, Y = A D and the parent
+// cotangent Y A^T hold one part (the other exactly zero), and the site cotangent
+// E Y is real. The real parts of the site cotangents -- and so the angle
+// gradients -- keep the four-product kernels' bits.
 template <bool REAL_A>
 __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradBwdMmaSmem &sm = *reinterpret_cast<GradBwdMmaSmem *>(smem_raw);
@@ -351,8 +358,8 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
       na.leaf = nb.leaf = -1;
       if (ca >= 0) na = p.nodes[ca];
       if (cbx >= 0) nb = p.nodes[cbx];
-      const double cfa = na.leaf >= 0 ? p.leaf_coef[na.leaf] : 0.0;
-      const double cfb = nb.leaf >= 0 ? p.leaf_coef[nb.leaf] : 0.0;
+      const double cfa = na.leaf >= 0 && !(REAL_A && (na.phase & 1)) ? p.leaf_coef[na.leaf] : 0.0;
+      const double cfb = nb.leaf >= 0 && !(REAL_A && (nb.phase & 1)) ? p.leaf_coef[nb.leaf] : 0.0;
       const cplx *bara = na.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + na.env_slot) * ENV_ELEMS : nullptr;
       const cplx *barb = nb.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + nb.env_slot) * ENV_ELEMS : nullptr;
       __syncwarp();   // the previous class's D is consumed
@@ -394,10 +401,14 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
           for (int ct = 0; ct < 4; ++ct) {
             const cplx a = af[ct >> 1][rt], d = df[ct];
-            dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
-            if (!REAL_A) dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
-            dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
-            if (!REAL_A) dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
+            if (REAL_A) {   // D of the parent's kind: its nonzero part, into yr
+              dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, odd ? d.y : d.x);
+            } else {
+              dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
+              dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
+              dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
+              dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
+            }
           }
       }
     }
@@ -409,7 +420,9 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int col = ct * 8 + 2 * t + j;
-          S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(yr[rt][ct][j], yi[rt][ct][j]);
+          cplx v = cmake(yr[rt][ct][j], yi[rt][ct][j]);
+          if (REAL_A) v = odd ? cmake(0.0, yr[rt][ct][j]) : cmake(yr[rt][ct][j], 0.0);
+          S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = v;
         }
     __syncwarp();
     // site cotangent: Abar_o += E Y_o (= S_src D_src summed over the classes, with S = E A)
@@ -426,10 +439,8 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
         for (int ct = 0; ct < 4; ++ct) {
           const cplx x = ef[rt], d = yf[ct];
           if (REAL_A) {
-            // even: re += Er Yr, im += Er Yi; odd: re += -Ei Yi, im += Ei Yr
-            const double xs = odd ? x.y : x.x;
-            dmma(abr[rt][ct][0], abr[rt][ct][1], odd ? -xs : xs, odd ? d.y : d.x);
-            dmma(abi[rt][ct][0], abi[rt][ct][1], xs, odd ? d.x : d.y);
+            // E and Y of one kind: even re += Er Yr, odd re += -Ei Yi (im stays zero)
+            dmma(abr[rt][ct][0], abr[rt][ct][1], odd ? -x.y : x.x, odd ? d.y : d.x);
           } else {
             dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
             dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
@@ -466,14 +477,29 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
           for (int ct = 0; ct < 2; ++ct) {
             if (rt == 1 && ct == 0) continue;
             // Y conj(A): re = Yr Ar + Yi Ai, im = Yi Ar - Yr Ai
-            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
-            if (!REAL_A) dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
-            dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
-            if (!REAL_A) dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
+            if (REAL_A) {   // Y of the parent's kind: its nonzero part, into orr
+              dmma(orr[rt][ct][0], orr[rt][ct][1], odd ? yf[rt].y : yf[rt].x, bf[ct].x);
+            } else {
+              dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
+              dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
+              dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
+              dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
+            }
           }
       }
       cplx *dst = grp.parent_slot >= 0 ? p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS
                                        : p.rootbar + ((size_t)b * p.n + p.s) * ENV_ELEMS;   // suffix root
+      if (REAL_A) {   // the parent's kind: orr is its real or its imaginary part
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              oi[rt][ct][j] = odd ? orr[rt][ct][j] : 0.0;
+              orr[rt][ct][j] = odd ? 0.0 : orr[rt][ct][j];
+            }
+      }
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
