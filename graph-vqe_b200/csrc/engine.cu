@@ -426,7 +426,7 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(grad_fwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradFwdMmaSmem));
   cudaFuncSetAttribute(grad_bwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(GradBwdMmaSmem));
+                       (int)sizeof(GradBwdRealSmem));
   if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT"))
     ctx->grad_mma = std::strcmp(v, "simt") == 0 ? 0 : std::strcmp(v, "dmma") == 0 ? 1 : 2;
   // VQEMPS_LEVEL_VARIANT pins the trie-level kernel (a name or an index); the
@@ -849,6 +849,10 @@ extern "C" int vqemps_set_hamiltonian(vqemps_ctx *ctx, const char *words, const 
         for (int k = first; k <= lastn; ++k) {
           const int c = h->nodes[h->node_off[s] + k].code;
           g.classes |= (c == 0 || c == 3) ? 1 : 2;
+        }
+        {
+          const DevNode &c0 = h->nodes[h->node_off[s] + first];
+          if ((c0.phase - (c0.code == 2 ? 1 : 0)) & 1) g.classes |= 4;   // odd parent phase
         }
         h->groups.push_back(g);
         // flop accounting with the actual bond dims (dl x dr site), as the

@@ -26,7 +26,8 @@ struct DevGroup {   // one trie parent with its children at the current level
   int32_t parent_slot;   // env slot of the parent in the previous level (-1: root)
   int32_t child_begin;   // first child node (index within the level)
   int32_t nchild;
-  int32_t classes;       // bit 0: an I or Z child, bit 1: an X or Y child
+  int32_t classes;       // bit 0: an I or Z child, bit 1: an X or Y child, bit 2: the
+                         // parent's phase (Y count) is odd (prefix and single-cut plans)
 };
 
 struct DevNode {    // one trie node

@@ -290,18 +290,6 @@ struct GradBwdMmaSmem {
   cplx D[GLEVEL_WARPS][2 * CHI * MMA_S_STRIDE];   // the class's D pair [d][k][c]
 };
 
-// REAL_A: a circuit of real gates. Its environments are i^k Er: real for even
-// phase k, imaginary for odd. A word with an odd number of Y's has the value
-// zero at every angle, and so has a pair closure of odd phase sum; their
-// cotangents reach only the imaginary parts of the site cotangents, which a
-// gradient with respect to real gate angles never reads. Left out (their leaf
-// weights taken as zero here, odd pairs masked by split_pair_bwd_kernel), every
-// cotangent is of its node's kind, like the environment, so each complex product
-// with the site tile, E or Y is one real product: D, Y = A D and the parent
-// cotangent Y A^T hold one part (the other exactly zero), and the site cotangent
-// E Y is real. The real parts of the site cotangents -- and so the angle
-// gradients -- keep the four-product kernels' bits.
-template <bool REAL_A>
 __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradBwdMmaSmem &sm = *reinterpret_cast<GradBwdMmaSmem *>(smem_raw);
   const int b = blockIdx.y;
@@ -339,11 +327,6 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
     const DevGroup grp = p.groups[gidx];
     int idx_child[4] = {-1, -1, -1, -1};
     for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
-    bool odd = false;   // REAL_A: E imaginary (the parent's phase, from its first child)
-    if (REAL_A) {
-      const DevNode n0 = p.nodes[grp.child_begin];
-      odd = ((n0.phase - (n0.code == 2 ? 1 : 0)) & 1) != 0;
-    }
     // Y_o = sum over classes of A_src(o) D_src(o)
     double yr[2][4][2], yi[2][4][2];
 #pragma unroll
@@ -358,8 +341,8 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
       na.leaf = nb.leaf = -1;
       if (ca >= 0) na = p.nodes[ca];
       if (cbx >= 0) nb = p.nodes[cbx];
-      const double cfa = na.leaf >= 0 && !(REAL_A && (na.phase & 1)) ? p.leaf_coef[na.leaf] : 0.0;
-      const double cfb = nb.leaf >= 0 && !(REAL_A && (nb.phase & 1)) ? p.leaf_coef[nb.leaf] : 0.0;
+      const double cfa = na.leaf >= 0 ? p.leaf_coef[na.leaf] : 0.0;
+      const double cfb = nb.leaf >= 0 ? p.leaf_coef[nb.leaf] : 0.0;
       const cplx *bara = na.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + na.env_slot) * ENV_ELEMS : nullptr;
       const cplx *barb = nb.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + nb.env_slot) * ENV_ELEMS : nullptr;
       __syncwarp();   // the previous class's D is consumed
@@ -401,14 +384,10 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
           for (int ct = 0; ct < 4; ++ct) {
             const cplx a = af[ct >> 1][rt], d = df[ct];
-            if (REAL_A) {   // D of the parent's kind: its nonzero part, into yr
-              dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, odd ? d.y : d.x);
-            } else {
-              dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
-              dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
-              dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
-              dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
-            }
+            dmma(yr[rt][ct][0], yr[rt][ct][1], a.x, d.x);
+            dmma(yr[rt][ct][0], yr[rt][ct][1], -a.y, d.y);
+            dmma(yi[rt][ct][0], yi[rt][ct][1], a.x, d.y);
+            dmma(yi[rt][ct][0], yi[rt][ct][1], a.y, d.x);
           }
       }
     }
@@ -420,9 +399,7 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
           const int col = ct * 8 + 2 * t + j;
-          cplx v = cmake(yr[rt][ct][j], yi[rt][ct][j]);
-          if (REAL_A) v = odd ? cmake(0.0, yr[rt][ct][j]) : cmake(yr[rt][ct][j], 0.0);
-          S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = v;
+          S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = cmake(yr[rt][ct][j], yi[rt][ct][j]);
         }
     __syncwarp();
     // site cotangent: Abar_o += E Y_o (= S_src D_src summed over the classes, with S = E A)
@@ -438,15 +415,10 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
 #pragma unroll
         for (int ct = 0; ct < 4; ++ct) {
           const cplx x = ef[rt], d = yf[ct];
-          if (REAL_A) {
-            // E and Y of one kind: even re += Er Yr, odd re += -Ei Yi (im stays zero)
-            dmma(abr[rt][ct][0], abr[rt][ct][1], odd ? -x.y : x.x, odd ? d.y : d.x);
-          } else {
-            dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
-            dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
-            dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
-            dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
-          }
+          dmma(abr[rt][ct][0], abr[rt][ct][1], x.x, d.x);
+          dmma(abr[rt][ct][0], abr[rt][ct][1], -x.y, d.y);
+          dmma(abi[rt][ct][0], abi[rt][ct][1], x.x, d.y);
+          dmma(abi[rt][ct][0], abi[rt][ct][1], x.y, d.x);
         }
     }
     __syncwarp();   // E is consumed: prefetch the next parent
@@ -477,29 +449,14 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
           for (int ct = 0; ct < 2; ++ct) {
             if (rt == 1 && ct == 0) continue;
             // Y conj(A): re = Yr Ar + Yi Ai, im = Yi Ar - Yr Ai
-            if (REAL_A) {   // Y of the parent's kind: its nonzero part, into orr
-              dmma(orr[rt][ct][0], orr[rt][ct][1], odd ? yf[rt].y : yf[rt].x, bf[ct].x);
-            } else {
-              dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
-              dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
-              dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
-              dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
-            }
+            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].x, bf[ct].x);
+            dmma(orr[rt][ct][0], orr[rt][ct][1], yf[rt].y, bf[ct].y);
+            dmma(oi[rt][ct][0], oi[rt][ct][1], yf[rt].y, bf[ct].x);
+            dmma(oi[rt][ct][0], oi[rt][ct][1], -yf[rt].x, bf[ct].y);
           }
       }
       cplx *dst = grp.parent_slot >= 0 ? p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS
                                        : p.rootbar + ((size_t)b * p.n + p.s) * ENV_ELEMS;   // suffix root
-      if (REAL_A) {   // the parent's kind: orr is its real or its imaginary part
-#pragma unroll
-        for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-          for (int ct = 0; ct < 2; ++ct)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              oi[rt][ct][j] = odd ? orr[rt][ct][j] : 0.0;
-              orr[rt][ct][j] = odd ? 0.0 : orr[rt][ct][j];
-            }
-      }
 #pragma unroll
       for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
@@ -534,17 +491,257 @@ __device__ __forceinline__ void grad_bwd_level_mma_body(const GradLevelParams &p
   }
 }
 
+// ---------------------------------------------------------------------------
+// backward level for a circuit of real gates. Its site tiles are real and its
+// environments i^k Er: real for an even phase k, imaginary for an odd one. A
+// word with an odd number of Y's has the value zero at every angle, and so has a
+// pair closure of odd phase sum; their cotangents reach only the imaginary parts
+// of the site cotangents, which a gradient with respect to real gate angles
+// never reads. Left out (their leaf weights taken as zero here, odd pairs masked
+// by split_pair_bwd_kernel), every cotangent is of its node's kind, like the
+// environment, so D, Y = A D and the parent cotangent Y A^T are of the parent's
+// kind (DevGroup::classes bit 2) and the site cotangent E Y is real: one real
+// DMMA product where grad_bwd_level_mma_body issues four, on the same operands in
+// the same order, so the real parts of the site cotangents -- and the angle
+// gradients -- keep that kernel's bits. Shared memory holds only the nonzero
+// parts (a double per element): 57 KB per CTA, three CTAs per SM, against
+// 106 KB for the complex tiles.
+// ---------------------------------------------------------------------------
+constexpr int GR_A_STRIDE = 36;   // real site tile, rows [a] of [i * 16 + c]
+constexpr int GR_E_STRIDE = 20;   // one part of the parent environment, 16 rows
+constexpr int GR_S_STRIDE = 20;   // one part of a [2][16][16] panel (D, Y)
+
+struct GradBwdRealSmem {
+  double A[CHI * GR_A_STRIDE];
+  double R[ENV_ELEMS];
+  double E[GLEVEL_WARPS][CHI * GR_E_STRIDE];
+  double S[GLEVEL_WARPS][2 * CHI * GR_S_STRIDE];   // Y panel; at the end the site cotangent panel
+  double D[GLEVEL_WARPS][2 * CHI * GR_S_STRIDE];
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+
+// The nonzero part of group grp's parent environment into E (cp.async), or of
+// the vacuum / a suffix root R_{s+1} (both real).
+__device__ __forceinline__ void grad_stage_parent_real(const GradLevelParams &p, int b, const DevGroup &grp, double *E,
+                                                       int lane) {
+  const double *src;
+  if (grp.parent_slot < 0 && !p.suffix) {
+    for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * GR_E_STRIDE + (e & 15)] = e == 0 ? 1.0 : 0.0;
+    return;
+  }
+  if (grp.parent_slot < 0)
+    src = reinterpret_cast<const double *>(p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS);
+  else
+    src = reinterpret_cast<const double *>(p.env_prev + (size_t)b * p.prev_stride +
+                                           (size_t)grp.parent_slot * ENV_ELEMS) + ((grp.classes & 4) ? 1 : 0);
+  for (int e = lane; e < ENV_ELEMS; e += 32) cp_async8(E + (e >> 4) * GR_E_STRIDE + (e & 15), src + 2 * e);
+}
+
+__device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &p, unsigned char *smem_raw) {
+  GradBwdRealSmem &sm = *reinterpret_cast<GradBwdRealSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) sm.A[(e >> 5) * GR_A_STRIDE + (e & 31)] = ag[e].x;
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) sm.R[e] = rg[e].x;
+  }
+  __syncthreads();
+  const double *A = sm.A;
+  const double *R = sm.R;
+  double *E = sm.E[warp];
+  double *S = sm.S[warp];
+  double *D = sm.D[warp];
+  const int g = lane >> 2, t = lane & 3;
+  // site cotangent panel of this warp (real): rows rt * 8 + g, cols ct * 8 + 2t + j of [Abar_0 | Abar_1]
+  double abr[2][4][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct) abr[rt][ct][0] = abr[rt][ct][1] = 0.0;
+  const int per_cta = GLEVEL_WARPS * GROUPS_PER_WARP;
+  const int g0 = blockIdx.x * per_cta;
+  const int g1 = min(g0 + per_cta, p.ngroups);
+  int gidx = g0 + warp;
+  if (gidx < g1) {
+    grad_stage_parent_real(p, b, p.groups[gidx], E, lane);
+    cp_async_commit();
+  }
+  for (; gidx < g1; gidx += GLEVEL_WARPS) {
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    const bool odd = (grp.classes & 4) != 0;
+    int idx_child[4] = {-1, -1, -1, -1};
+    for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
+    // Y_o = sum over classes of A_src(o) D_src(o), one part
+    double yr[2][4][2];
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) yr[rt][ct][0] = yr[rt][ct][1] = 0.0;
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      const int ca = idx_child[cls == 0 ? 0 : 1], cbx = idx_child[cls == 0 ? 3 : 2];
+      DevNode na{}, nb{};
+      na.env_slot = nb.env_slot = -1;
+      na.leaf = nb.leaf = -1;
+      if (ca >= 0) na = p.nodes[ca];
+      if (cbx >= 0) nb = p.nodes[cbx];
+      // leaves of odd phase are left out (zero value at every angle)
+      const double cfa = na.leaf >= 0 && !(na.phase & 1) ? p.leaf_coef[na.leaf] : 0.0;
+      const double cfb = nb.leaf >= 0 && !(nb.phase & 1) ? p.leaf_coef[nb.leaf] : 0.0;
+      const cplx *bara = na.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + na.env_slot) * ENV_ELEMS : nullptr;
+      const cplx *barb = nb.env_slot >= 0 ? p.bar_cur + ((size_t)b * p.maxslot + nb.env_slot) * ENV_ELEMS : nullptr;
+      __syncwarp();   // the previous class's D is consumed
+      for (int e = lane; e < ENV_ELEMS; e += 32) {
+        // the complex D entries of the four-product kernels, of which the part of
+        // the parent's kind is kept (the other is zero)
+        const cplx rc = cmake(R[e], -0.0);
+        cplx xa = cscale(rc, cfa), xb = cscale(rc, cfb);
+        if (bara) xa = cadd(xa, bara[e]);
+        if (barb) xb = cadd(xb, barb[e]);
+        cplx d0, d1;
+        if (cls == 0) {
+          d0 = cadd(xa, xb);
+          d1 = csub(xa, xb);
+        } else {
+          const cplx ixb = cmake(-xb.y, xb.x);
+          d0 = cadd(xa, ixb);
+          d1 = csub(xa, ixb);
+        }
+        D[(e >> 4) * GR_S_STRIDE + (e & 15)] = odd ? d0.y : d0.x;
+        D[(CHI + (e >> 4)) * GR_S_STRIDE + (e & 15)] = odd ? d1.y : d1.x;
+      }
+      __syncwarp();
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        double af[2][2], df[4];
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+          const int src = cls == 0 ? o : 1 - o;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt) af[o][rt] = A[(rt * 8 + g) * GR_A_STRIDE + src * CHI + ks * 4 + t];
+        }
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) {
+          const int src = cls == 0 ? (ct >> 1) : 1 - (ct >> 1);
+          df[ct] = D[(src * CHI + ks * 4 + t) * GR_S_STRIDE + (ct & 1) * 8 + g];
+        }
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) dmma(yr[rt][ct][0], yr[rt][ct][1], af[ct >> 1][rt], df[ct]);
+      }
+    }
+    // Y panel (one part) into S: Y_i[row][c] at S[(i * CHI + row) * GR_S_STRIDE + c]
+#pragma unroll
+    for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int col = ct * 8 + 2 * t + j;
+          S[((col >> 4) * CHI + rt * 8 + g) * GR_S_STRIDE + (col & 15)] = yr[rt][ct][j];
+        }
+    __syncwarp();
+    // site cotangent (real): even Abar += Er Yr, odd Abar += -Ei Yi
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+      double ef[2], yf[4];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt) {
+        const double x = E[(rt * 8 + g) * GR_E_STRIDE + ks * 4 + t];
+        ef[rt] = odd ? -x : x;
+      }
+#pragma unroll
+      for (int ct = 0; ct < 4; ++ct) yf[ct] = S[((ct >> 1) * CHI + ks * 4 + t) * GR_S_STRIDE + (ct & 1) * 8 + g];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) dmma(abr[rt][ct][0], abr[rt][ct][1], ef[rt], yf[ct]);
+    }
+    __syncwarp();   // E is consumed: prefetch the next parent
+    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent_real(p, b, p.groups[gidx + GLEVEL_WARPS], E, lane);
+    cp_async_commit();
+    if (p.s > 0) {
+      // parent cotangent Ebar = sum_i Y_i A_i^T, tiles (0,0), (0,1), (1,1); the
+      // (1,0) tile is the conjugate transpose of (0,1)
+      double o[2][2][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) o[rt][ct][0] = o[rt][ct][1] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 8; ++ks) {
+        const int kk = ks * 4 + t;            // (i, k) = (kk >> 4, kk & 15)
+        double yf[2], bf[2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) yf[rt] = S[((kk >> 4) * CHI + rt * 8 + g) * GR_S_STRIDE + (kk & 15)];
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) bf[ct] = A[(ct * 8 + g) * GR_A_STRIDE + kk];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            if (rt == 1 && ct == 0) continue;
+            dmma(o[rt][ct][0], o[rt][ct][1], yf[rt], bf[ct]);
+          }
+      }
+      cplx *dst = grp.parent_slot >= 0 ? p.bar_prev + ((size_t)b * p.maxslot + grp.parent_slot) * ENV_ELEMS
+                                       : p.rootbar + ((size_t)b * p.n + p.s) * ENV_ELEMS;   // suffix root
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j)
+            dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = odd ? cmake(0.0, o[rt][ct][j]) : cmake(o[rt][ct][j], 0.0);
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+        dst[(8 + 2 * t + j) * CHI + g] = odd ? cmake(0.0, -o[0][1][j]) : cmake(o[0][1][j], -0.0);
+    }
+    __syncwarp();   // S / D are rewritten by the next group
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // fixed-order combination of the warps' site cotangent panels (times 2)
+  double *panel = sm.S[warp];     // 640 >= 512 entries, one per site element
+#pragma unroll
+  for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+    for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+        const int col = ct * 8 + 2 * t + j;
+        panel[((rt * 8 + g) * 2 + (col >> 4)) * CHI + (col & 15)] = 2.0 * abr[rt][ct][j];
+      }
+  __syncthreads();
+  cplx *dst = p.partial + ((size_t)b * gridDim.x + blockIdx.x) * SITE_ELEMS;
+  for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) {
+    double acc = sm.S[0][e];
+    for (int w = 1; w < GLEVEL_WARPS; ++w) acc += sm.S[w][e];
+    dst[e] = cmake(acc, 0.0);
+  }
+}
+
 __global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
 grad_bwd_level_mma_kernel(GradLevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_bwd_level_mma_body<false>(p, smem_raw);
+  grad_bwd_level_mma_body(p, smem_raw);
 }
 
-// Backward gradient level for a circuit of real gates (real site tiles).
-__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
+// Backward gradient level for a circuit of real gates (real site tiles,
+// one-part shared tiles; three CTAs per SM).
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 3)
 grad_bwd_level_real_a_kernel(GradLevelParams p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_bwd_level_mma_body<true>(p, smem_raw);
+  grad_bwd_level_real_body(p, smem_raw);
 }
 
 }  // namespace vqemps
