@@ -424,7 +424,7 @@ extern "C" int vqemps_create(int device, int max_bond, double abs_cut, double re
   cudaFuncSetAttribute(grad_fwd_level_mma3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradFwdMmaSmem));
   cudaFuncSetAttribute(grad_fwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(GradFwdMmaSmem));
+                       (int)sizeof(GradFwdRealSmem));
   cudaFuncSetAttribute(grad_bwd_level_real_a_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)sizeof(GradBwdRealSmem));
   if (const char *v = std::getenv("VQEMPS_GRAD_VARIANT"))

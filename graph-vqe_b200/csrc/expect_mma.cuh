@@ -278,46 +278,6 @@ __device__ __forceinline__ void class_tiles(const cplx *A, int xoff, const cplx 
   }
 }
 
-// class_tiles of KIND 2 when, besides X, the panel y holds values of one kind:
-// all real (odd false) or all imaginary (odd true) -- an environment i^k Er of
-// a circuit of real gates times real site tiles. One real product, into re or
-// im; the other part is the exact zero KIND 2 would have summed (same bits).
-template <bool SKIP10>
-__device__ __forceinline__ void class_tiles_pure(const cplx *A, int xoff, const cplx *S, int y, double (&re)[2][2][2],
-                                                 double (&im)[2][2][2], int g, int t, bool odd) {
-  double acc[2][2][2];
-#pragma unroll
-  for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-    for (int ct = 0; ct < 2; ++ct) acc[rt][ct][0] = acc[rt][ct][1] = 0.0;
-  const double *Ad = reinterpret_cast<const double *>(A);
-  const double *Sd = reinterpret_cast<const double *>(S) + (odd ? 1 : 0);
-#pragma unroll
-  for (int ks = 0; ks < 4; ++ks) {
-    double x[2], yv[2];
-#pragma unroll
-    for (int rt = 0; rt < 2; ++rt) x[rt] = Ad[2 * ((ks * 4 + t) * MMA_A_STRIDE + xoff + rt * 8 + g)];
-#pragma unroll
-    for (int ct = 0; ct < 2; ++ct) yv[ct] = Sd[2 * ((y * CHI + ks * 4 + t) * MMA_S_STRIDE + ct * 8 + g)];
-#pragma unroll
-    for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-      for (int ct = 0; ct < 2; ++ct) {
-        if (SKIP10 && rt == 1 && ct == 0) continue;
-        dmma(acc[rt][ct][0], acc[rt][ct][1], x[rt], yv[ct]);
-      }
-  }
-#pragma unroll
-  for (int rt = 0; rt < 2; ++rt)
-#pragma unroll
-    for (int ct = 0; ct < 2; ++ct)
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        re[rt][ct][j] = odd ? 0.0 : acc[rt][ct][j];
-        im[rt][ct][j] = odd ? acc[rt][ct][j] : 0.0;
-      }
-}
-
 // GAUSS selects the complex product: false = four real DMMA products
 // (Re = XrYr - XiYi, Im = XrYi + XiYr); true = Gauss's three-product form
 // k1 = Yr (Xr + Xi), k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi), Re = k1 - k3,

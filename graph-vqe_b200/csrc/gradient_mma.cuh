@@ -41,11 +41,9 @@ __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int 
 // KIND 1 (Gauss): three real products per complex product (k1 = Yr (Xr + Xi),
 // k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2); KIND 0:
 // four; KIND 2: A real (a circuit of real gates), two -- the four-product sums
-// without their exact-zero terms, so the same bits; KIND 3: A real and E of one
-// kind, i^k Er (real for even k, imaginary for odd: odd = k & 1), one -- KIND 2
-// without the products of E's zero part (same bits again).
+// without their exact-zero terms, so the same bits.
 template <int KIND = 0>
-__device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t, bool odd = false) {
+__device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
   constexpr bool GAUSS = KIND == 1;
   double sr[2][4][2], si[2][4][2], s3[GAUSS ? 2 : 1][4][2];
 #pragma unroll
@@ -77,8 +75,6 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
         } else if constexpr (KIND == 2) {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
-        } else if constexpr (KIND == 3) {
-          dmma(sr[rt][ct][0], sr[rt][ct][1], odd ? ei : er, pf[ct].x);
         } else {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
@@ -97,7 +93,6 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
         const int col = ct * 8 + 2 * t + j;
         cplx v;
         if constexpr (GAUSS) v = cmake(sr[rt][ct][j] - s3[rt][ct][j], sr[rt][ct][j] + si[rt][ct][j]);
-        else if constexpr (KIND == 3) v = odd ? cmake(0.0, sr[rt][ct][j]) : cmake(sr[rt][ct][j], 0.0);
         else v = cmake(sr[rt][ct][j], si[rt][ct][j]);
         S[((col >> 4) * CHI + rt * 8 + g) * MMA_S_STRIDE + (col & 15)] = v;
       }
@@ -134,13 +129,7 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
-    // KIND 3: the parent's phase k (from its first child) says whether E is real or imaginary
-    bool odd = false;
-    if constexpr (KIND == 3) {
-      const DevNode n0 = p.nodes[grp.child_begin];
-      odd = ((n0.phase - (n0.code == 2 ? 1 : 0)) & 1) != 0;
-    }
-    mma_panel_EA<KIND>(E, A, S, g, t, odd);
+    mma_panel_EA<KIND>(E, A, S, g, t);
     __syncwarp();   // E is dead and S complete: prefetch the next parent
     if (gidx + GLEVEL_WARPS < g1) grad_stage_parent(p, b, gidx + GLEVEL_WARPS, E, lane);
     cp_async_commit();
@@ -150,16 +139,10 @@ __device__ __forceinline__ void grad_fwd_level_mma_body(const GradLevelParams &p
       // X/Y: t1 = A_1^H S_0 = t0^H through the S panel (as level_mma_pf_body).
       double ar[2][2][2], ai[2][2][2], br[2][2][2], bi[2][2][2];
       if (cls == 0) {
-        if constexpr (KIND == 3) {
-          class_tiles_pure<true>(A, 0, S, 0, ar, ai, g, t, odd);
-          class_tiles_pure<true>(A, CHI, S, 1, br, bi, g, t, odd);
-        } else {
-          class_tiles<KIND, true>(A, 0, S, 0, ar, ai, g, t);
-          class_tiles<KIND, true>(A, CHI, S, 1, br, bi, g, t);
-        }
+        class_tiles<KIND, true>(A, 0, S, 0, ar, ai, g, t);
+        class_tiles<KIND, true>(A, CHI, S, 1, br, bi, g, t);
       } else {
-        if constexpr (KIND == 3) class_tiles_pure<false>(A, 0, S, 1, ar, ai, g, t, odd);
-        else class_tiles<KIND, false>(A, 0, S, 1, ar, ai, g, t);
+        class_tiles<KIND, false>(A, 0, S, 1, ar, ai, g, t);
         __syncwarp();
 #pragma unroll
         for (int rt = 0; rt < 2; ++rt)
@@ -263,14 +246,7 @@ grad_fwd_level_mma3_kernel(GradLevelParams p) {
   grad_fwd_level_mma_body<1>(p, smem_raw);
 }
 
-// Forward gradient level for a circuit of real gates: real site tiles and
-// environments i^k Er, one real product per complex one where the four-product
-// kernel issues four (its bits).
-__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
-grad_fwd_level_real_a_kernel(GradLevelParams p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  grad_fwd_level_mma_body<3>(p, smem_raw);
-}
+
 
 // ---------------------------------------------------------------------------
 // backward level on DMMA. Per group (parent E, site A = [A_0 A_1]):
@@ -728,6 +704,219 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
     for (int w = 1; w < GLEVEL_WARPS; ++w) acc += sm.S[w][e];
     dst[e] = cmake(acc, 0.0);
   }
+}
+
+// ---------------------------------------------------------------------------
+// forward level for a circuit of real gates on one-part shared tiles: the
+// real-site products of grad_fwd_level_mma_body<2> without the products of
+// E's zero part (E and S = E A are of the parent's kind, DevGroup::classes bit
+// 2: one real DMMA product per complex one), only the nonzero parts of E and S
+// in shared memory, and the children's complex values and leaf sums formed by
+// the same expressions (same bits). 55 KB per CTA against 85 KB.
+// ---------------------------------------------------------------------------
+struct GradFwdRealSmem {
+  double A[CHI * GR_A_STRIDE];
+  cplx R[ENV_ELEMS];
+  double E[GLEVEL_WARPS][CHI * GR_E_STRIDE];
+  double S[GLEVEL_WARPS][2 * CHI * GR_S_STRIDE];
+  cplx L[GLEVEL_WARPS][ENV_ELEMS];
+};
+
+__device__ __forceinline__ void grad_fwd_level_real_body(const GradLevelParams &p, unsigned char *smem_raw) {
+  GradFwdRealSmem &sm = *reinterpret_cast<GradFwdRealSmem *>(smem_raw);
+  const int b = blockIdx.y;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  {
+    const cplx *ag = p.sites + ((size_t)b * p.n + p.s) * SITE_ELEMS;
+    const cplx *rg = p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS;
+    for (int e = threadIdx.x; e < SITE_ELEMS; e += GLEVEL_WARPS * 32) sm.A[(e >> 5) * GR_A_STRIDE + (e & 31)] = ag[e].x;
+    for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) sm.R[e] = rg[e];
+    for (int e = lane; e < ENV_ELEMS; e += 32) sm.L[warp][e] = cmake(0, 0);
+  }
+  __syncthreads();
+  const double *A = sm.A;
+  const cplx *R = sm.R;
+  double *E = sm.E[warp];
+  double *S = sm.S[warp];
+  cplx *L = sm.L[warp];
+  const int g = lane >> 2, t = lane & 3;
+  const int per_cta = GLEVEL_WARPS * GROUPS_PER_WARP;
+  const int g0 = blockIdx.x * per_cta;
+  const int g1 = min(g0 + per_cta, p.ngroups);
+  int gidx = g0 + warp;
+  if (gidx < g1) {
+    grad_stage_parent_real(p, b, p.groups[gidx], E, lane);
+    cp_async_commit();
+  }
+  for (; gidx < g1; gidx += GLEVEL_WARPS) {
+    cp_async_wait<0>();
+    __syncwarp();
+    const DevGroup grp = p.groups[gidx];
+    const bool odd = (grp.classes & 4) != 0;
+    // S = E [A_0 | A_1], one part
+    {
+      double sacc[2][4][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) sacc[rt][ct][0] = sacc[rt][ct][1] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        double ef[2], pf[4];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) ef[rt] = E[(rt * 8 + g) * GR_E_STRIDE + ks * 4 + t];
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct) pf[ct] = A[(ks * 4 + t) * GR_A_STRIDE + ct * 8 + g];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 4; ++ct) dmma(sacc[rt][ct][0], sacc[rt][ct][1], ef[rt], pf[ct]);
+      }
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 4; ++ct)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            const int col = ct * 8 + 2 * t + j;
+            S[((col >> 4) * CHI + rt * 8 + g) * GR_S_STRIDE + (col & 15)] = sacc[rt][ct][j];
+          }
+    }
+    __syncwarp();   // E is dead and S complete: prefetch the next parent
+    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent_real(p, b, p.groups[gidx + GLEVEL_WARPS], E, lane);
+    cp_async_commit();
+    for (int cls = 0; cls < 2; ++cls) {
+      if (!(grp.classes & (1 << cls))) continue;
+      // one part of t0 = A_x^H S_y (and of t1): I/Z t0 = A_0^T S_0, t1 = A_1^T S_1
+      // over tiles (0,0), (0,1), (1,1); X/Y t0 = A_0^T S_1 over four tiles and
+      // t1 = t0^H through the panel
+      double a[2][2][2], c[2][2][2];
+#pragma unroll
+      for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) a[rt][ct][0] = a[rt][ct][1] = c[rt][ct][0] = c[rt][ct][1] = 0.0;
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        double x0[2], x1[2], y0[2], y1[2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt) {
+          x0[rt] = A[(ks * 4 + t) * GR_A_STRIDE + rt * 8 + g];
+          x1[rt] = A[(ks * 4 + t) * GR_A_STRIDE + CHI + rt * 8 + g];
+        }
+#pragma unroll
+        for (int ct = 0; ct < 2; ++ct) {
+          y0[ct] = S[(ks * 4 + t) * GR_S_STRIDE + ct * 8 + g];
+          y1[ct] = S[(CHI + ks * 4 + t) * GR_S_STRIDE + ct * 8 + g];
+        }
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct) {
+            if (cls == 0) {
+              if (rt == 1 && ct == 0) continue;
+              dmma(a[rt][ct][0], a[rt][ct][1], x0[rt], y0[ct]);
+              dmma(c[rt][ct][0], c[rt][ct][1], x1[rt], y1[ct]);
+            } else {
+              dmma(a[rt][ct][0], a[rt][ct][1], x0[rt], y1[ct]);
+            }
+          }
+      }
+      if (cls == 1) {
+        __syncwarp();   // the panel is consumed: t0 goes into its place
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = 0; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) S[(rt * 8 + g) * GR_S_STRIDE + ct * 8 + 2 * t + j] = a[rt][ct][j];
+        __syncwarp();
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) c[rt][ct][j] = S[(ct * 8 + 2 * t + j) * GR_S_STRIDE + rt * 8 + g];
+      }
+      for (int ci = 0; ci < grp.nchild; ++ci) {
+        const DevNode node = p.nodes[grp.child_begin + ci];
+        const bool iz = (node.code == 0 || node.code == 3);
+        if (iz != (cls == 0)) continue;
+        cplx out[2][2][2];
+#pragma unroll
+        for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+          for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              // the complex t0, t1 of the four-product kernels (zero part exact)
+              const double pa = a[rt][ct][j], pc = c[rt][ct][j];
+              const cplx t0 = odd ? cmake(0.0, pa) : cmake(pa, 0.0);
+              const cplx t1 = cls == 0 ? (odd ? cmake(0.0, pc) : cmake(pc, 0.0))
+                                       : (odd ? cmake(0.0, -pc) : cmake(pc, -0.0));
+              if (node.code == 0 || node.code == 1) out[rt][ct][j] = cadd(t0, t1);
+              else if (node.code == 3) out[rt][ct][j] = csub(t0, t1);
+              else { const cplx d = csub(t1, t0); out[rt][ct][j] = cmake(-d.y, d.x); }
+            }
+        // out[1][0][j]: the (1,0)-tile element this lane owns, [8 + 2t + j][g]
+        out[1][0][0] = cconj(out[0][1][0]);
+        out[1][0][1] = cconj(out[0][1][1]);
+        if (node.env_slot >= 0) {
+          cplx *dst = p.env_cur + (size_t)b * p.cur_stride + (size_t)node.env_slot * ENV_ELEMS;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+#pragma unroll
+          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = out[1][0][j];
+        }
+        if (node.leaf >= 0 && p.leaf_work) {
+          const double cf = p.leaf_coef[node.leaf];
+          double v = 0.0;
+#pragma unroll
+          for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+            for (int ct = rt; ct < 2; ++ct)
+#pragma unroll
+              for (int j = 0; j < 2; ++j) {
+                const int idx = (rt * 8 + g) * CHI + ct * 8 + 2 * t + j;
+                const cplx rv = R[idx];
+                v += out[rt][ct][j].x * rv.x - out[rt][ct][j].y * rv.y;
+                L[idx] = cadd(L[idx], cscale(out[rt][ct][j], cf));
+              }
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {   // the (1,0) tile
+            const int idx = (8 + 2 * t + j) * CHI + g;
+            const cplx rv = R[idx];
+            v += out[1][0][j].x * rv.x - out[1][0][j].y * rv.y;
+            L[idx] = cadd(L[idx], cscale(out[1][0][j], cf));
+          }
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) p.leafval[(size_t)b * p.nleaf + node.leaf] = v;
+        }
+      }
+    }
+    __syncwarp();   // S is rewritten by the next parent
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  if (!p.leaf_work) return;
+  cplx *dst = p.partial + ((size_t)b * gridDim.x + blockIdx.x) * ENV_ELEMS;
+  for (int e = threadIdx.x; e < ENV_ELEMS; e += GLEVEL_WARPS * 32) {
+    cplx acc = sm.L[0][e];
+    for (int w = 1; w < GLEVEL_WARPS; ++w) acc = cadd(acc, sm.L[w][e]);
+    dst[e] = acc;
+  }
+}
+
+// Forward gradient level for a circuit of real gates: real site tiles and
+// environments i^k Er, one real product per complex one where the four-product
+// kernel issues four (its bits); one-part shared tiles, three CTAs per SM.
+__global__ void __launch_bounds__(GLEVEL_WARPS * 32, 3)
+grad_fwd_level_real_a_kernel(GradLevelParams p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  grad_fwd_level_real_body(p, smem_raw);
 }
 
 __global__ void __launch_bounds__(GLEVEL_WARPS * 32, 2)
