@@ -180,6 +180,11 @@ struct GradLevelParams {
   // parent cotangent (the cotangent of R_{s+1}) to rootbar[b][s].
   int suffix;
   cplx *rootbar;            // B x n x ENV_ELEMS
+  // Real-gate kernels (grad_*_level_real_a_kernel): an environment of one kind
+  // is stored as its nonzero part only, ENV_ELEMS doubles at the start of its
+  // slot, unless env_complex is set for the level written -- the split plan's
+  // cut levels, which the pair kernels read.
+  int env_complex;
 };
 
 struct GradFwdSmem {

@@ -500,22 +500,25 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
 }
 
-// The nonzero part of group grp's parent environment into E (cp.async), or of
-// the vacuum / a suffix root R_{s+1} (both real).
+// The nonzero part of group grp's parent environment into E (cp.async): a
+// parent of the previous level is stored as that part (ENV_ELEMS doubles; no
+// cut level is a parent), the vacuum and a suffix root R_{s+1} are real.
 __device__ __forceinline__ void grad_stage_parent_real(const GradLevelParams &p, int b, const DevGroup &grp, double *E,
                                                        int lane) {
-  const double *src;
   if (grp.parent_slot < 0 && !p.suffix) {
     for (int e = lane; e < ENV_ELEMS; e += 32) E[(e >> 4) * GR_E_STRIDE + (e & 15)] = e == 0 ? 1.0 : 0.0;
     return;
   }
-  if (grp.parent_slot < 0)
-    src = reinterpret_cast<const double *>(p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS);
-  else
-    src = reinterpret_cast<const double *>(p.env_prev + (size_t)b * p.prev_stride +
-                                           (size_t)grp.parent_slot * ENV_ELEMS) + ((grp.classes & 4) ? 1 : 0);
-  for (int e = lane; e < ENV_ELEMS; e += 32) cp_async8(E + (e >> 4) * GR_E_STRIDE + (e & 15), src + 2 * e);
+  if (grp.parent_slot < 0) {
+    const double *src = reinterpret_cast<const double *>(p.right + ((size_t)b * (p.n + 1) + p.s + 1) * ENV_ELEMS);
+    for (int e = lane; e < ENV_ELEMS; e += 32) cp_async8(E + (e >> 4) * GR_E_STRIDE + (e & 15), src + 2 * e);
+    return;
+  }
+  const double *src =
+      reinterpret_cast<const double *>(p.env_prev + (size_t)b * p.prev_stride + (size_t)grp.parent_slot * ENV_ELEMS);
+  for (int e = 2 * lane; e < ENV_ELEMS; e += 64) cp_async16(E + (e >> 4) * GR_E_STRIDE + (e & 15), src + e);
 }
+
 
 __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &p, unsigned char *smem_raw) {
   GradBwdRealSmem &sm = *reinterpret_cast<GradBwdRealSmem *>(smem_raw);
@@ -862,14 +865,28 @@ __device__ __forceinline__ void grad_fwd_level_real_body(const GradLevelParams &
         out[1][0][1] = cconj(out[0][1][1]);
         if (node.env_slot >= 0) {
           cplx *dst = p.env_cur + (size_t)b * p.cur_stride + (size_t)node.env_slot * ENV_ELEMS;
+          if (p.env_complex) {
 #pragma unroll
-          for (int rt = 0; rt < 2; ++rt)
+            for (int rt = 0; rt < 2; ++rt)
 #pragma unroll
-            for (int ct = rt; ct < 2; ++ct)
+              for (int ct = rt; ct < 2; ++ct)
 #pragma unroll
-              for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
+                for (int j = 0; j < 2; ++j) dst[(rt * 8 + g) * CHI + ct * 8 + 2 * t + j] = out[rt][ct][j];
 #pragma unroll
-          for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = out[1][0][j];
+            for (int j = 0; j < 2; ++j) dst[(8 + 2 * t + j) * CHI + g] = out[1][0][j];
+          } else {   // the nonzero part (the child's kind)
+            double *dd = reinterpret_cast<double *>(dst);
+            const bool oc = (node.phase & 1) != 0;
+#pragma unroll
+            for (int rt = 0; rt < 2; ++rt)
+#pragma unroll
+              for (int ct = rt; ct < 2; ++ct)
+                *reinterpret_cast<double2 *>(dd + (rt * 8 + g) * CHI + ct * 8 + 2 * t) =
+                    oc ? make_double2(out[rt][ct][0].y, out[rt][ct][1].y)
+                       : make_double2(out[rt][ct][0].x, out[rt][ct][1].x);
+#pragma unroll
+            for (int j = 0; j < 2; ++j) dd[(8 + 2 * t + j) * CHI + g] = oc ? out[1][0][j].y : out[1][0][j].x;
+          }
         }
         if (node.leaf >= 0 && p.leaf_work) {
           const double cf = p.leaf_coef[node.leaf];
