@@ -495,6 +495,11 @@ struct GradBwdRealSmem {
   double D[GLEVEL_WARPS][2 * CHI * GR_S_STRIDE];
 };
 
+// Hint: bring the 128-byte line at p into L2 (no effect on results).
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p));
+}
+
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
@@ -646,7 +651,14 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
         for (int ct = 0; ct < 4; ++ct) dmma(abr[rt][ct][0], abr[rt][ct][1], ef[rt], yf[ct]);
     }
     __syncwarp();   // E is consumed: prefetch the next parent
-    if (gidx + GLEVEL_WARPS < g1) grad_stage_parent_real(p, b, p.groups[gidx + GLEVEL_WARPS], E, lane);
+    // and the slot of one of its children (lanes 8c .. 8c + 7: child c), whose
+    // cotangent is warmed into L2 below, after the parent cotangent product
+    int next_slot = -1;
+    if (gidx + GLEVEL_WARPS < g1) {
+      const DevGroup gn = p.groups[gidx + GLEVEL_WARPS];
+      grad_stage_parent_real(p, b, gn, E, lane);
+      if ((lane >> 3) < gn.nchild) next_slot = p.nodes[gn.child_begin + (lane >> 3)].env_slot;
+    }
     cp_async_commit();
     if (p.s > 0) {
       // parent cotangent Ebar = sum_i Y_i A_i^T, tiles (0,0), (0,1), (1,1); the
@@ -684,6 +696,11 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
 #pragma unroll
       for (int j = 0; j < 2; ++j)
         dst[(8 + 2 * t + j) * CHI + g] = odd ? cmake(0.0, -o[0][1][j]) : cmake(o[0][1][j], -0.0);
+    }
+    if (next_slot >= 0) {   // 4 KB cotangent = 32 lines, four per lane of the child's eight
+      const char *line = reinterpret_cast<const char *>(p.bar_cur + ((size_t)b * p.maxslot + next_slot) * ENV_ELEMS);
+#pragma unroll
+      for (int l = 0; l < 4; ++l) prefetch_l2(line + ((lane & 7) * 4 + l) * 128);
     }
     __syncwarp();   // S / D are rewritten by the next group
   }
