@@ -552,17 +552,31 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
   const int g0 = blockIdx.x * per_cta;
   const int g1 = min(g0 + per_cta, p.ngroups);
   int gidx = g0 + warp;
+  // the next group's child records, one per lane (at most four), loaded when its
+  // parent is staged and read back with shuffles
+  DevNode nd_next{};
   if (gidx < g1) {
-    grad_stage_parent_real(p, b, p.groups[gidx], E, lane);
+    const DevGroup gf = p.groups[gidx];
+    grad_stage_parent_real(p, b, gf, E, lane);
+    if (lane < gf.nchild) nd_next = p.nodes[gf.child_begin + lane];
     cp_async_commit();
   }
+  auto shfl_node = [&](const DevNode &v, int src) {
+    DevNode r;
+    r.code = __shfl_sync(0xffffffffu, v.code, src);
+    r.env_slot = __shfl_sync(0xffffffffu, v.env_slot, src);
+    r.leaf = __shfl_sync(0xffffffffu, v.leaf, src);
+    r.phase = __shfl_sync(0xffffffffu, v.phase, src);
+    return r;
+  };
   for (; gidx < g1; gidx += GLEVEL_WARPS) {
     cp_async_wait<0>();
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
     const bool odd = (grp.classes & 4) != 0;
-    int idx_child[4] = {-1, -1, -1, -1};
-    for (int ci = 0; ci < grp.nchild; ++ci) idx_child[p.nodes[grp.child_begin + ci].code] = grp.child_begin + ci;
+    const DevNode nd = nd_next;
+    int idx_child[4] = {-1, -1, -1, -1};   // child (lane of nd) of each Pauli code
+    for (int ci = 0; ci < grp.nchild; ++ci) idx_child[__shfl_sync(0xffffffffu, nd.code, ci)] = ci;
     // Y_o = sum over classes of A_src(o) D_src(o), one part
     double yr[2][4][2];
 #pragma unroll
@@ -575,8 +589,9 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
       DevNode na{}, nb{};
       na.env_slot = nb.env_slot = -1;
       na.leaf = nb.leaf = -1;
-      if (ca >= 0) na = p.nodes[ca];
-      if (cbx >= 0) nb = p.nodes[cbx];
+      const DevNode ra = shfl_node(nd, ca < 0 ? 0 : ca), rb = shfl_node(nd, cbx < 0 ? 0 : cbx);
+      if (ca >= 0) na = ra;
+      if (cbx >= 0) nb = rb;
       // leaves of odd phase are left out (zero value at every angle)
       const double cfa = na.leaf >= 0 && !(na.phase & 1) ? p.leaf_coef[na.leaf] : 0.0;
       const double cfb = nb.leaf >= 0 && !(nb.phase & 1) ? p.leaf_coef[nb.leaf] : 0.0;
@@ -651,13 +666,16 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
         for (int ct = 0; ct < 4; ++ct) dmma(abr[rt][ct][0], abr[rt][ct][1], ef[rt], yf[ct]);
     }
     __syncwarp();   // E is consumed: prefetch the next parent
-    // and the slot of one of its children (lanes 8c .. 8c + 7: child c), whose
-    // cotangent is warmed into L2 below, after the parent cotangent product
-    int next_slot = -1;
-    if (gidx + GLEVEL_WARPS < g1) {
+    // and its child records; the cotangents of its children (lanes 8c .. 8c + 7:
+    // child c) are warmed into L2 below, after the parent cotangent product
+    const bool has_next = gidx + GLEVEL_WARPS < g1;
+    int next_nchild = 0;
+    if (has_next) {
       const DevGroup gn = p.groups[gidx + GLEVEL_WARPS];
       grad_stage_parent_real(p, b, gn, E, lane);
-      if ((lane >> 3) < gn.nchild) next_slot = p.nodes[gn.child_begin + (lane >> 3)].env_slot;
+      next_nchild = gn.nchild;
+      nd_next = DevNode{};
+      if (lane < gn.nchild) nd_next = p.nodes[gn.child_begin + lane];
     }
     cp_async_commit();
     if (p.s > 0) {
@@ -696,6 +714,11 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
 #pragma unroll
       for (int j = 0; j < 2; ++j)
         dst[(8 + 2 * t + j) * CHI + g] = odd ? cmake(0.0, -o[0][1][j]) : cmake(o[0][1][j], -0.0);
+    }
+    int next_slot = -1;
+    if (has_next) {
+      const int sl = __shfl_sync(0xffffffffu, nd_next.env_slot, lane >> 3);
+      if ((lane >> 3) < next_nchild) next_slot = sl;
     }
     if (next_slot >= 0) {   // 4 KB cotangent = 32 lines, four per lane of the child's eight
       const char *line = reinterpret_cast<const char *>(p.bar_cur + ((size_t)b * p.maxslot + next_slot) * ENV_ELEMS);
@@ -773,6 +796,10 @@ __device__ __forceinline__ void grad_fwd_level_real_body(const GradLevelParams &
     __syncwarp();
     const DevGroup grp = p.groups[gidx];
     const bool odd = (grp.classes & 4) != 0;
+    // the children's node records, one per lane (at most four), loaded while the
+    // S product runs and read back with shuffles
+    DevNode nd{};
+    if (lane < grp.nchild) nd = p.nodes[grp.child_begin + lane];
     // S = E [A_0 | A_1], one part
     {
       double sacc[2][4][2];
@@ -858,7 +885,11 @@ __device__ __forceinline__ void grad_fwd_level_real_body(const GradLevelParams &
             for (int j = 0; j < 2; ++j) c[rt][ct][j] = S[(ct * 8 + 2 * t + j) * GR_S_STRIDE + rt * 8 + g];
       }
       for (int ci = 0; ci < grp.nchild; ++ci) {
-        const DevNode node = p.nodes[grp.child_begin + ci];
+        DevNode node;
+        node.code = __shfl_sync(0xffffffffu, nd.code, ci);
+        node.env_slot = __shfl_sync(0xffffffffu, nd.env_slot, ci);
+        node.leaf = __shfl_sync(0xffffffffu, nd.leaf, ci);
+        node.phase = __shfl_sync(0xffffffffu, nd.phase, ci);
         const bool iz = (node.code == 0 || node.code == 3);
         if (iz != (cls == 0)) continue;
         cplx out[2][2][2];
