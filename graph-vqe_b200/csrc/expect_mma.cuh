@@ -223,10 +223,7 @@ __device__ __forceinline__ void stage_parent_padded(const LevelParams &p, int b,
 // Class-product tiles of conj(A_x)^T S_y (x = column offset 0 or CHI of the A
 // panel, y = panel half) over the 8 x 8 output tiles (rt, ct); SKIP10 leaves
 // the (1,0) tile out. KIND 1 (Gauss): k1 = Yr (Xr - Xi), k2 = Xr (Yi - Yr),
-// k3 = -Xi (Yr + Yi), Re = k1 - k3, Im = k1 + k2; KIND 0: four real products;
-// KIND 2: X real (a circuit of real gates: site tiles with zero imaginary
-// parts), two real products -- the four-product sums without their exact-zero
-// terms, so the same bits.
+// k3 = -Xi (Yr + Yi), Re = k1 - k3, Im = k1 + k2; KIND 0: four real products.
 template <int KIND, bool SKIP10>
 __device__ __forceinline__ void class_tiles(const cplx *A, int xoff, const cplx *S, int y, double (&re)[2][2][2],
                                             double (&im)[2][2][2], int g, int t) {
@@ -253,9 +250,6 @@ __device__ __forceinline__ void class_tiles(const cplx *A, int xoff, const cplx 
           dmma(re[rt][ct][0], re[rt][ct][1], x[rt].x - x[rt].y, yv[ct].x);
           dmma(im[rt][ct][0], im[rt][ct][1], x[rt].x, yv[ct].y - yv[ct].x);
           dmma(k3[rt][ct][0], k3[rt][ct][1], -x[rt].y, yv[ct].x + yv[ct].y);
-        } else if constexpr (KIND == 2) {
-          dmma(re[rt][ct][0], re[rt][ct][1], x[rt].x, yv[ct].x);
-          dmma(im[rt][ct][0], im[rt][ct][1], x[rt].x, yv[ct].y);
         } else {
           dmma(re[rt][ct][0], re[rt][ct][1], x[rt].x, yv[ct].x);
           dmma(re[rt][ct][0], re[rt][ct][1], x[rt].y, yv[ct].y);

@@ -40,8 +40,7 @@ __device__ __forceinline__ void grad_stage_parent(const GradLevelParams &p, int 
 // S panel [S_0 | S_1] = E [A_0 | A_1] (16 x 32, K = 16) into padded S[i][row][col];
 // KIND 1 (Gauss): three real products per complex product (k1 = Yr (Xr + Xi),
 // k2 = Xr (Yi - Yr), k3 = Xi (Yr + Yi); Re = k1 - k3, Im = k1 + k2); KIND 0:
-// four; KIND 2: A real (a circuit of real gates), two -- the four-product sums
-// without their exact-zero terms, so the same bits.
+// four.
 template <int KIND = 0>
 __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx *S, int g, int t) {
   constexpr bool GAUSS = KIND == 1;
@@ -72,9 +71,6 @@ __device__ __forceinline__ void mma_panel_EA(const cplx *E, const cplx *A, cplx 
           dmma(sr[rt][ct][0], sr[rt][ct][1], er + ei, pf[ct].x);                 // k1
           dmma(si[rt][ct][0], si[rt][ct][1], er, pf[ct].y - pf[ct].x);           // k2
           dmma(s3[rt][ct][0], s3[rt][ct][1], ei, pf[ct].x + pf[ct].y);           // k3
-        } else if constexpr (KIND == 2) {
-          dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
-          dmma(si[rt][ct][0], si[rt][ct][1], ei, pf[ct].x);
         } else {
           dmma(sr[rt][ct][0], sr[rt][ct][1], er, pf[ct].x);
           dmma(sr[rt][ct][0], sr[rt][ct][1], nei, pf[ct].y);
@@ -751,11 +747,12 @@ __device__ __forceinline__ void grad_bwd_level_real_body(const GradLevelParams &
 
 // ---------------------------------------------------------------------------
 // forward level for a circuit of real gates on one-part shared tiles: the
-// real-site products of grad_fwd_level_mma_body<2> without the products of
-// E's zero part (E and S = E A are of the parent's kind, DevGroup::classes bit
-// 2: one real DMMA product per complex one), only the nonzero parts of E and S
-// in shared memory, and the children's complex values and leaf sums formed by
-// the same expressions (same bits). 55 KB per CTA against 85 KB.
+// products of grad_fwd_level_mma_body<0> without the exact-zero terms of the
+// real site tile and of E's zero part (E and S = E A are of the parent's kind,
+// DevGroup::classes bit 2: one real DMMA product per complex one), only the
+// nonzero parts of E and S in shared memory, and the children's complex values
+// and leaf sums formed by the same expressions (same bits). 55 KB per CTA
+// against 85 KB.
 // ---------------------------------------------------------------------------
 struct GradFwdRealSmem {
   double A[CHI * GR_A_STRIDE];
