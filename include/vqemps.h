@@ -140,7 +140,9 @@ int vqemps_energy_grad_batch(vqemps_ctx *ctx, int handle, const double *theta_de
 int vqemps_set_grad_checkpoint(vqemps_ctx *ctx, int every);
 /* Gradient level kernels (no reference counterpart): 0 = SIMT FMA kernels,
  * 1 = FP64 DMMA tensor-core kernels, 2 = DMMA with Gauss's three-product complex
- * multiply in the forward levels (default). All give the same values to
+ * multiply in the forward levels (default); for a circuit of real gates, 2 runs
+ * the real-gate DMMA kernels (one real product per complex one; energies and
+ * angle gradients equal variant 1's bit for bit). All give the same values to
  * rounding; VQEMPS_GRAD_VARIANT (simt, dmma, dmma3) selects one at creation. */
 int vqemps_set_grad_variant(vqemps_ctx *ctx, int variant);
 
